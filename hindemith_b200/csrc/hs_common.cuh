@@ -1,0 +1,67 @@
+// hs_common.cuh -- shared helpers of libhsflow: status plumbing, argument checks,
+// launch helpers and the canonical Horn-Schunck stencil tables.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdarg>
+#include <cstdio>
+
+#include "../../include/hsflow.h"
+
+namespace hs {
+
+// Thread-local one-line detail of the last failing call (hs_last_error()).
+void set_error(const char *fmt, ...);
+void clear_error();
+
+#define HS_FAIL(code, ...)               \
+    do {                                 \
+        ::hs::set_error(__VA_ARGS__);    \
+        return (code);                   \
+    } while (0)
+
+#define HS_CUDA_CHECK(expr)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (expr);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            HS_FAIL(HS_ERR_CUDA, "%s failed: %s", #expr, cudaGetErrorString(e_));        \
+    } while (0)
+
+// Check the result of the kernel launch just issued.
+#define HS_LAUNCH_CHECK(what)                                                            \
+    do {                                                                                 \
+        cudaError_t e_ = cudaGetLastError();                                             \
+        if (e_ != cudaSuccess)                                                           \
+            HS_FAIL(HS_ERR_CUDA, "launch of %s failed: %s", what, cudaGetErrorString(e_)); \
+    } while (0)
+
+inline bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Plane geometry checks shared by every entry point.
+inline hs_status check_plane_geometry(int H, int W, int ld) {
+    if (H < 1 || W < 1) HS_FAIL(HS_ERR_INVALID_ARG, "H=%d W=%d must be >= 1", H, W);
+    if (ld < W) HS_FAIL(HS_ERR_INVALID_ARG, "ld=%d < W=%d", ld, W);
+    if (ld % 4 != 0) HS_FAIL(HS_ERR_ALIGNMENT, "ld=%d is not a multiple of 4 floats", ld);
+    if ((long long)H * ld > (1LL << 40)) HS_FAIL(HS_ERR_INVALID_ARG, "plane too large");
+    return HS_OK;
+}
+
+inline hs_status check_plane(const void *p, const char *name) {
+    if (!p) HS_FAIL(HS_ERR_INVALID_ARG, "%s is NULL", name);
+    if (!aligned16(p)) HS_FAIL(HS_ERR_ALIGNMENT, "%s is not 16-byte aligned", name);
+    return HS_OK;
+}
+
+inline size_t plane_bytes(int H, int ld) { return sizeof(float) * (size_t)H * (size_t)ld; }
+
+// Number of SMs of the current device (cached per device).
+int sm_count();
+
+// Canonical Horn-Schunck stencils.  Average: 3x3 without centre, corners 1/12, edges 1/6,
+// taps row-major (dy = -1, 0, +1; dx = -1, 0, +1).  Derivatives: taps (0,0) (1,0) (0,1) (1,1).
+constexpr float kAvgCorner = (float)(1.0 / 12.0);
+constexpr float kAvgEdge = (float)(1.0 / 6.0);
+
+}  // namespace hs

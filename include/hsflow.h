@@ -1,0 +1,133 @@
+/*
+ * hsflow.h -- C ABI of libhsflow.so, the B200 (sm_100a) implementation of the
+ * Horn-Schunck stencil path of chick/hindemith.
+ *
+ * Conventions for every entry point:
+ *   - Images are dense FP32 planes, row-major, x (width) fastest: element (x, y) is
+ *     at p[x + y * ld]  (the reference's index x + y*W, Types/Array2D.cpp:302).
+ *     H, W >= 1; ld >= W, ld % 4 == 0; every plane pointer is 16-byte aligned.
+ *   - Pointers named in/out/u/v/I0/... are DEVICE pointers owned by the caller.
+ *     Stencil taps (weights/offx/offy) are HOST arrays, copied into the launch.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream).  Nothing blocks
+ *     the host; errors found by argument checks are returned before any launch,
+ *     launch errors are returned from the launching call.
+ *   - Every call returns an hs_status; hs_last_error() gives a one-line detail
+ *     for the calling thread.  No C++ exception crosses this boundary.
+ *   - Scratch memory is the caller's: functions that need it take
+ *     (workspace, workspace_bytes) and say how much through *_workspace_bytes().
+ *
+ * Each function cites the reference interface it replaces (paths inside
+ * chick/hindemith).
+ */
+#ifndef HSFLOW_H
+#define HSFLOW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define HS_API __attribute__((visibility("default")))
+#else
+#define HS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hs_status {
+    HS_OK = 0,
+    HS_ERR_INVALID_ARG = 1,   /* null pointer, non-positive size, bad op code, ... */
+    HS_ERR_ALIGNMENT = 2,     /* ld % 4 != 0 or a plane not 16-byte aligned */
+    HS_ERR_WORKSPACE = 3,     /* workspace missing or smaller than required */
+    HS_ERR_CUDA = 4,          /* a CUDA runtime call or launch failed */
+    HS_ERR_TIMEOUT = 5,       /* a bounded device-side wait gave up */
+    HS_ERR_UNSUPPORTED = 6,   /* valid request this build does not implement */
+    HS_ERR_NO_DEVICE = 7      /* no usable sm_100 device */
+} hs_status;
+
+/* Binary operator codes, the reference's op names (Array2DOp.cpp:36-51). */
+typedef enum hs_binop { HS_OP_ADD = 0, HS_OP_SUB = 1, HS_OP_MUL = 2, HS_OP_DIV = 3 } hs_binop;
+
+#define HS_MAX_TAPS 64
+#define HS_MAX_SWEEPS_PER_PASS 8
+
+/* Tuning of the sweep kernels.  Zero-initialise for the defaults. */
+typedef struct hs_config {
+    int sweeps_per_pass;  /* temporal-blocking depth T (1..8) = sweeps per HBM pass; 0 = default */
+    int rows_per_segment; /* rows each warp streams per work item; 0 = default */
+    int fast_math;        /* 0 (default): the reference program's operation order, one
+                             rounding per operation -- bit-identical to the reference's
+                             FP32 semantics for any T;  1: factored stencil, fused
+                             multiply-adds and a per-pixel reciprocal, within 1e-4 */
+    float avg_edge;       /* weight of the 4 edge taps of the 3x3 average; 0 = 1/6 */
+    float avg_corner;     /* weight of the 4 corner taps; 0 = 1/12 (both 0 = the HS stencil) */
+    int reserved[3];      /* must be zero */
+} hs_config;
+
+/* ---- library ---------------------------------------------------------------- */
+HS_API const char *hs_status_string(hs_status status);
+HS_API const char *hs_last_error(void);
+HS_API int hs_version(void);
+
+/* ---- structured-grid operations (the reference's operator plugins) ------------ */
+
+/* out = S * in: out(x,y) = sum_d w[d] * in(clamp(x+offx[d]), clamp(y+offy[d])), summed
+ * from 0 in tap order, one rounding per operation.  1 <= ntaps <= HS_MAX_TAPS.
+ * Replaces Stencil2DMVMSetupLaunch + Stencil2DMVMElementLevel::compile
+ * (Operations/StructuredGrid/Stencil2DMVM.cpp:62, :34-59).  in != out. */
+HS_API hs_status hs_stencil2d(const float *weights, const int *offx, const int *offy, int ntaps,
+                       const float *in, float *out, int H, int W, int ld, void *stream);
+
+/* a = b op c (Operations/DenseLinearAlgebra/Array2DOp.cpp:27-118). */
+HS_API hs_status hs_array2d_op(int op, const float *b, const float *c, float *a, int H, int W, int ld,
+                        void *stream);
+/* a = b op s (Array2DScalarOp.cpp:29-118). */
+HS_API hs_status hs_array2d_scalar_op(int op, const float *b, float s, float *a, int H, int W, int ld,
+                               void *stream);
+/* a = s op b (ScalarArray2DOp.cpp:29-119). */
+HS_API hs_status hs_scalar_array2d_op(int op, float s, const float *b, float *a, int H, int W, int ld,
+                               void *stream);
+/* a = b (Array2DCopy.cpp:23-93). */
+HS_API hs_status hs_array2d_copy(const float *b, float *a, int H, int W, int ld, void *stream);
+
+/* ---- Horn-Schunck ----------------------------------------------------------- */
+
+/* 2x2x2 derivatives in one pass: Ix = Dx*I0 + Dx*I1, Iy = Dy*I0 + Dy*I1,
+ * It = Dt*I1 - Dt*I0 with Dx, Dy, Dt the 4-tap stencils over {0,1}^2 (weights -1/4,
+ * +1/4 for Dx/Dy, 1/4 for Dt) and clamp-to-edge taps.  Bit-identical to the
+ * reference program's FP32 result.  Replaces the fused derivative strand the
+ * reference builds from Stencil2DMVM + Array2DOp (Stencil2DMVM.cpp:34-59,
+ * Array2DOp.cpp:27-53, fused by fusion.cpp:113-303). */
+HS_API hs_status hs_derivs(const float *I0, const float *I1, int H, int W, int ld, float *Ix,
+                    float *Iy, float *It, void *stream);
+
+/* Scratch needed by hs_sweeps: two planes (the ping-pong copy of u, v). */
+HS_API size_t hs_sweeps_workspace_bytes(int H, int W, int ld);
+
+/* `iters` Jacobi sweeps in place on (u, v), from their current contents:
+ *   ubar = A*u; vbar = A*v          (A: 3x3 clamp-to-edge average, 1/6 edges, 1/12 corners)
+ *   t = (Ix*ubar + Iy*vbar + It) / (alpha2 + Ix*Ix + Iy*Iy)
+ *   u = ubar - Ix*t; v = vbar - Iy*t
+ * T sweeps run per pass over HBM (cfg->sweeps_per_pass).  iters >= 0.
+ * Replaces the Iterator's host loop (execute.cpp:35-45) over the two fused sweep
+ * kernels (Stencil2DMVM.cpp:34-59 + Array2DOp/Array2DScalarOp/Array2DCopy chains). */
+HS_API hs_status hs_sweeps(const float *Ix, const float *Iy, const float *It, int H, int W, int ld,
+                    float alpha2, int iters, float *u, float *v, void *workspace,
+                    size_t workspace_bytes, const hs_config *cfg, void *stream);
+
+/* Scratch needed by hs_forward: five planes (Ix, Iy, It and the ping-pong copy). */
+HS_API size_t hs_forward_workspace_bytes(int H, int W, int ld);
+
+/* The plain per-pair drop-in: derivatives, u = v = 0, `iters` sweeps with
+ * alpha2 = alpha * alpha (FP32).  Replaces backend.run for a compiled Horn-Schunck
+ * program (backend.cpp:320-638) end to end on the device. */
+HS_API hs_status hs_forward(const float *I0, const float *I1, int H, int W, int ld, float alpha,
+                     int iters, float *u, float *v, void *workspace, size_t workspace_bytes,
+                     const hs_config *cfg, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HSFLOW_H */

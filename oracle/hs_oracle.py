@@ -1,0 +1,261 @@
+"""CPU oracle for the Horn-Schunck stencil path (TEST INFRASTRUCTURE ONLY).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py``
+use this module, always as the checker.  The product package never imports it.
+
+Two restatements of the reference's semantics live here:
+
+* NumPy functions (``stencil2d``, ``hs_derivs``, ``hs_sweeps``, ``hs_forward``,
+  ``warp``).  With ``dtype=np.float32`` they do one IEEE-rounded FP32 operation at a
+  time, in the order the reference program performs them, so they match the
+  reference's FP32 results bit for bit.  With ``dtype=np.float64`` they are the
+  accuracy reference.
+* ctypes wrappers (``c_*``) over ``oracle/hs_oracle.c``, the same restatement in C
+  with OpenMP, fast enough for full-size checks and the CPU baseline.
+
+Reference anchors (paths inside chick/hindemith):
+  Stencil2DMVM.cpp:34-59      clamp-to-edge tap loop, accumulate from 0 in tap order
+  Types/Array2D.cpp:302,333   element index x + y*W (x = last NumPy axis)
+  Array2DOp.cpp:27-53         a = b op c, op in {+,-,*,/}
+  Array2DScalarOp.cpp:29-55   a = b op *scalar
+  ScalarArray2DOp.cpp:29-55   a = *scalar op b
+  WarpImg2D.cpp:33-75         bilinear backward warp, source pixel when out of bounds
+  hlib.py:173-191             NumPy Stencil.__mul__ (edge padding; symmetric stencils)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libhsoracle.so")
+
+# Canonical Horn-Schunck stencils, tap order (offx, offy).  Identical tables live in the
+# CUDA sources and in hindemith_b200.stencils; the tests check that they agree.
+AVG_OFFX = np.array([-1, 0, 1, -1, 1, -1, 0, 1], dtype=np.int32)
+AVG_OFFY = np.array([-1, -1, -1, 0, 0, 1, 1, 1], dtype=np.int32)
+AVG_W = np.array([1 / 12 if (ox != 0 and oy != 0) else 1 / 6
+                  for ox, oy in zip(AVG_OFFX, AVG_OFFY)], dtype=np.float32)
+D_OFFX = np.array([0, 1, 0, 1], dtype=np.int32)
+D_OFFY = np.array([0, 0, 1, 1], dtype=np.int32)
+DX_W = np.array([-0.25, 0.25, -0.25, 0.25], dtype=np.float32)
+DY_W = np.array([-0.25, -0.25, 0.25, 0.25], dtype=np.float32)
+DT_W = np.array([0.25, 0.25, 0.25, 0.25], dtype=np.float32)
+
+
+# ---------------------------------------------------------------- NumPy restatement
+
+def stencil2d(w, offx, offy, x, dtype=np.float32):
+    """y[r, c] = sum_d w[d] * x[clamp(r + offy[d]), clamp(c + offx[d])], from 0, tap order.
+
+    Stencil2DMVM.cpp:37-48.  Each product and each sum rounds to ``dtype``.
+    """
+    x = np.asarray(x, dtype=dtype)
+    H, W = x.shape
+    rows = np.arange(H)
+    cols = np.arange(W)
+    acc = np.zeros((H, W), dtype=dtype)
+    for d in range(len(w)):
+        rr = np.clip(rows + int(offy[d]), 0, H - 1)
+        cc = np.clip(cols + int(offx[d]), 0, W - 1)
+        acc = acc + dtype(w[d]) * x[rr][:, cc]
+    return acc
+
+
+def stencil2d_transpose(w, offx, offy, x, dtype=np.float64):
+    """S^T x for the clamp-to-edge stencil S (scatter form; small sizes only)."""
+    x = np.asarray(x, dtype=dtype)
+    H, W = x.shape
+    out = np.zeros((H, W), dtype=dtype)
+    rows = np.arange(H)
+    cols = np.arange(W)
+    for d in range(len(w)):
+        rr = np.clip(rows + int(offy[d]), 0, H - 1)
+        cc = np.clip(cols + int(offx[d]), 0, W - 1)
+        np.add.at(out, (rr[:, None], cc[None, :]), dtype(w[d]) * x)
+    return out
+
+
+def hs_derivs(I0, I1, dtype=np.float32):
+    """Ix = Dx*I0 + Dx*I1, Iy = Dy*I0 + Dy*I1, It = Dt*I1 - Dt*I0."""
+    Ix = stencil2d(DX_W, D_OFFX, D_OFFY, I0, dtype) + stencil2d(DX_W, D_OFFX, D_OFFY, I1, dtype)
+    Iy = stencil2d(DY_W, D_OFFX, D_OFFY, I0, dtype) + stencil2d(DY_W, D_OFFX, D_OFFY, I1, dtype)
+    It = stencil2d(DT_W, D_OFFX, D_OFFY, I1, dtype) - stencil2d(DT_W, D_OFFX, D_OFFY, I0, dtype)
+    return Ix, Iy, It
+
+
+def hs_sweeps(Ix, Iy, It, alpha2, iters, u, v, dtype=np.float32):
+    """`iters` Jacobi sweeps: ubar = A*u; vbar = A*v;
+    t = (Ix*ubar + Iy*vbar + It) / (alpha2 + Ix*Ix + Iy*Iy); u = ubar - Ix*t; v = vbar - Iy*t.
+    """
+    Ix, Iy, It = (np.asarray(a, dtype=dtype) for a in (Ix, Iy, It))
+    u = np.array(u, dtype=dtype)
+    v = np.array(v, dtype=dtype)
+    a2 = dtype(alpha2)
+    den = a2 + Ix * Ix + Iy * Iy
+    for _ in range(iters):
+        ubar = stencil2d(AVG_W, AVG_OFFX, AVG_OFFY, u, dtype)
+        vbar = stencil2d(AVG_W, AVG_OFFX, AVG_OFFY, v, dtype)
+        t = (Ix * ubar + Iy * vbar + It) / den
+        u = ubar - Ix * t
+        v = vbar - Iy * t
+    return u, v
+
+
+def hs_forward(I0, I1, alpha, iters, dtype=np.float32):
+    """Derivatives, u = v = 0, `iters` sweeps; alpha2 = alpha * alpha in ``dtype``."""
+    Ix, Iy, It = hs_derivs(I0, I1, dtype)
+    z = np.zeros(np.shape(I0), dtype=dtype)
+    a = dtype(alpha)
+    return hs_sweeps(Ix, Iy, It, a * a, iters, z, z, dtype)
+
+
+def warp(src, ox, oy):
+    """WarpImg2D.cpp:33-75 with its FP32/FP64 roundings (see hs_oracle.c)."""
+    src = np.asarray(src, dtype=np.float32)
+    ox = np.asarray(ox, dtype=np.float32)
+    oy = np.asarray(oy, dtype=np.float32)
+    H, W = src.shape
+    mx = np.trunc(ox).astype(np.int64)
+    my = np.trunc(oy).astype(np.int64)
+    xf = (ox - mx.astype(np.float32)).astype(np.float32)
+    yf = (oy - my.astype(np.float32)).astype(np.float32)
+    negx = ox < 0
+    negy = oy < 0
+    mx = np.where(negx, mx - 1, mx)
+    my = np.where(negy, my - 1, my)
+    xf = np.where(negx, (1.0 + xf.astype(np.float64)).astype(np.float32), xf)
+    yf = np.where(negy, (1.0 + yf.astype(np.float64)).astype(np.float32), yf)
+    X, Y = np.meshgrid(np.arange(W), np.arange(H))
+    ok = (X + mx >= 0) & (X + mx + 1 < W) & (Y + my >= 0) & (Y + my + 1 < H)
+    bx = np.where(ok, X + mx, 0)
+    by = np.where(ok, Y + my, 0)
+    bx1 = np.minimum(bx + 1, W - 1)
+    by1 = np.minimum(by + 1, H - 1)
+    xd = xf.astype(np.float64)
+    yd = yf.astype(np.float64)
+    s = src.astype(np.float64)
+    o = np.zeros((H, W), dtype=np.float32)
+    o = (o + s[by, bx] * (1.0 - xd) * (1.0 - yd)).astype(np.float32)
+    o = (o + s[by, bx1] * xd * (1.0 - yd)).astype(np.float32)
+    o = (o + s[by1, bx] * (1.0 - xd) * yd).astype(np.float32)
+    o = (o + s[by1, bx1] * xd * yd).astype(np.float32)
+    return np.where(ok, o, src).astype(np.float32)
+
+
+# ---------------------------------------------------------------- C restatement
+
+_lib = None
+
+
+def build():
+    """Compile hs_oracle.c into oracle/_build/libhsoracle.so."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+        c_int, c_float, c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
+        L.hso_num_threads.restype = c_int
+        L.hso_stencil2d_f32.argtypes = [f32p, i32p, i32p, c_int, f32p, f32p, c_int, c_int]
+        L.hso_stencil2d_f64.argtypes = [f64p, i32p, i32p, c_int, f64p, f64p, c_int, c_int]
+        L.hso_stencil2d_transpose_f64.argtypes = [f64p, i32p, i32p, c_int, f64p, f64p, c_int, c_int]
+        L.hso_hs_derivs_f32.argtypes = [f32p, f32p, c_int, c_int, f32p, f32p, f32p]
+        L.hso_hs_derivs_f64.argtypes = [f64p, f64p, c_int, c_int, f64p, f64p, f64p]
+        L.hso_hs_sweeps_f32.argtypes = [f32p, f32p, f32p, c_int, c_int, c_float, c_int, f32p, f32p]
+        L.hso_hs_sweeps_f64.argtypes = [f64p, f64p, f64p, c_int, c_int, c_double, c_int, f64p, f64p]
+        L.hso_hs_forward_f32.argtypes = [f32p, f32p, c_int, c_int, c_float, c_int, f32p, f32p]
+        L.hso_hs_forward_f64.argtypes = [f64p, f64p, c_int, c_int, c_double, c_int, f64p, f64p]
+        L.hso_warp_f32.argtypes = [f32p, f32p, f32p, c_int, c_int, f32p]
+        for name in ("hso_hs_sweeps_f32", "hso_hs_sweeps_f64", "hso_hs_forward_f32",
+                     "hso_hs_forward_f64"):
+            getattr(L, name).restype = c_int
+        _lib = L
+    return _lib
+
+
+def _c32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def c_num_threads():
+    return lib().hso_num_threads()
+
+
+def c_stencil2d(w, offx, offy, x, dtype=np.float32):
+    x = np.ascontiguousarray(x, dtype=dtype)
+    H, W = x.shape
+    out = np.empty_like(x)
+    ox = np.ascontiguousarray(offx, dtype=np.int32)
+    oy = np.ascontiguousarray(offy, dtype=np.int32)
+    if dtype == np.float32:
+        lib().hso_stencil2d_f32(_c32(w), ox, oy, len(ox), x, out, H, W)
+    else:
+        lib().hso_stencil2d_f64(_c64(w), ox, oy, len(ox), x, out, H, W)
+    return out
+
+
+def c_stencil2d_transpose(w, offx, offy, x):
+    x = _c64(x)
+    H, W = x.shape
+    out = np.empty_like(x)
+    ox = np.ascontiguousarray(offx, dtype=np.int32)
+    oy = np.ascontiguousarray(offy, dtype=np.int32)
+    lib().hso_stencil2d_transpose_f64(_c64(w), ox, oy, len(ox), x, out, H, W)
+    return out
+
+
+def c_hs_derivs(I0, I1, dtype=np.float32):
+    conv = _c32 if dtype == np.float32 else _c64
+    I0, I1 = conv(I0), conv(I1)
+    H, W = I0.shape
+    Ix, Iy, It = (np.empty_like(I0) for _ in range(3))
+    fn = lib().hso_hs_derivs_f32 if dtype == np.float32 else lib().hso_hs_derivs_f64
+    fn(I0, I1, H, W, Ix, Iy, It)
+    return Ix, Iy, It
+
+
+def c_hs_sweeps(Ix, Iy, It, alpha2, iters, u, v, dtype=np.float32):
+    conv = _c32 if dtype == np.float32 else _c64
+    Ix, Iy, It = conv(Ix), conv(Iy), conv(It)
+    u = conv(u).copy()
+    v = conv(v).copy()
+    H, W = Ix.shape
+    fn = lib().hso_hs_sweeps_f32 if dtype == np.float32 else lib().hso_hs_sweeps_f64
+    if fn(Ix, Iy, It, H, W, alpha2, int(iters), u, v) != 0:
+        raise MemoryError("oracle sweep allocation failed")
+    return u, v
+
+
+def c_hs_forward(I0, I1, alpha, iters, dtype=np.float32):
+    conv = _c32 if dtype == np.float32 else _c64
+    I0, I1 = conv(I0), conv(I1)
+    H, W = I0.shape
+    u = np.empty_like(I0)
+    v = np.empty_like(I0)
+    fn = lib().hso_hs_forward_f32 if dtype == np.float32 else lib().hso_hs_forward_f64
+    if fn(I0, I1, H, W, alpha, int(iters), u, v) != 0:
+        raise MemoryError("oracle forward allocation failed")
+    return u, v
+
+
+def c_warp(src, ox, oy):
+    src, ox, oy = _c32(src), _c32(ox), _c32(oy)
+    H, W = src.shape
+    out = np.empty_like(src)
+    lib().hso_warp_f32(src, ox, oy, H, W, out)
+    return out
