@@ -1,0 +1,114 @@
+"""Autotuner for the sweep kernel's temporal-blocking depth T and segment length.
+
+For an image shape it times candidate (T, rows_per_segment) pairs with CUDA events on
+the device (a fixed number of sweeps over synthetic coefficient planes of that shape)
+and keeps the fastest.  Results are cached per (device name, H, W, ld, mode) in memory
+and, when HS_AUTOTUNE_CACHE names a file, in that JSON file.
+"""
+from __future__ import annotations
+
+import json
+import os
+import threading
+from typing import Dict, Tuple
+
+_cache: Dict[str, Tuple[int, int]] = {}
+_lock = threading.Lock()
+
+T_CANDIDATES = (1, 2, 3, 4, 5, 6, 8)
+
+
+def _seg_candidates(H: int, W: int, T: int):
+    out = {0}
+    for L in (16, 32, 64, 128, 256):
+        if L < H:
+            out.add(L)
+    return sorted(out)
+
+
+def _key(dev_name, H, W, ld, fast_math):
+    return f"{dev_name}|{H}x{W}|ld{ld}|{'fast' if fast_math else 'exact'}"
+
+
+def _file():
+    return os.environ.get("HS_AUTOTUNE_CACHE")
+
+
+def _load_file():
+    path = _file()
+    if path and os.path.exists(path):
+        try:
+            with open(path) as f:
+                for k, v in json.load(f).items():
+                    _cache.setdefault(k, tuple(v))
+        except (OSError, ValueError):
+            pass
+
+
+def _save_file():
+    path = _file()
+    if path:
+        try:
+            with open(path, "w") as f:
+                json.dump({k: list(v) for k, v in _cache.items()}, f, indent=1)
+        except OSError:
+            pass
+
+
+def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=3):
+    import torch
+
+    from . import _lib as L
+    from . import device as D
+
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=fast_math)
+    D.hs_sweeps(Ix, Iy, It, 1.0, T, u, v, cfg)  # warm-up, first-launch attributes
+    best = float("inf")
+    for _ in range(reps):
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record()
+        D.hs_sweeps(Ix, Iy, It, 1.0, sweeps, u, v, cfg)
+        b.record()
+        b.synchronize()
+        best = min(best, a.elapsed_time(b))
+    return best
+
+
+def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
+                      candidates=T_CANDIDATES) -> Tuple[int, int]:
+    """(sweeps_per_pass, rows_per_segment) fastest on the current device for HxW."""
+    import torch
+
+    from . import device as D
+
+    dev_name = torch.cuda.get_device_name()
+    key = _key(dev_name, H, W, ld, fast_math)
+    with _lock:
+        if not _cache:
+            _load_file()
+        if key in _cache:
+            return _cache[key]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    planes = D.empty_planes(5, H, W)
+    for p in planes:
+        p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
+    Ix, Iy, It, u, v = planes
+    sweeps = 120  # a multiple of every candidate T
+    results = []
+    for T in candidates:
+        for seg in _seg_candidates(H, W, T):
+            ms = time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps)
+            results.append((ms, T, seg))
+    results.sort()
+    best = (results[0][1], results[0][2])
+    with _lock:
+        _cache[key] = best
+        _save_file()
+    return best
+
+
+def clear():
+    with _lock:
+        _cache.clear()

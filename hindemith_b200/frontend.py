@@ -293,10 +293,12 @@ def _split_mult(e):
     return None
 
 
-def _match_hs_body(final: Dict[str, Any], assigned, invariant) -> Optional[dict]:
-    """Find U, V with U' = A*U - Ix*t, V' = A*V - Iy*t,
-    t = ((Ix*(A*U) + Iy*(A*V)) + It) / den, all of Ix, Iy, It, den loop-invariant."""
-    arrays = [n for n in assigned if isinstance(final.get(n), tuple)]
+def _match_hs_body(final: Dict[str, Any], assigned, invariant):
+    """Yield every (U, V) with U' = A*U - Ix*t, V' = A*V - Iy*t,
+    t = ((Ix*(A*U) + Iy*(A*V)) + It) / den, all of Ix, Iy, It, den loop-invariant.
+    The update is symmetric in (U, Ix) <-> (V, Iy); the caller picks the orientation
+    whose denominator association matches the kernel's."""
+    arrays = sorted(n for n in assigned if isinstance(final.get(n), tuple))
     for U, V in itertools.permutations(arrays, 2):
         eu, ev = final[U], final[V]
         if not (_is_op(eu, "Sub") and _is_op(ev, "Sub")):
@@ -323,9 +325,8 @@ def _match_hs_body(final: Dict[str, Any], assigned, invariant) -> Optional[dict]
         want = ("op", "Add", ("op", "Add", ("op", "Mult", ix, su), ("op", "Mult", iy, sv)), it)
         if _canon(num) != _canon(want):
             continue
-        return {"U": U, "V": V, "A": su[1], "Ix": ix[1], "Iy": iy[1], "It": it[1],
-                "den": den[1]}
-    return None
+        yield {"U": U, "V": V, "A": su[1], "Ix": ix[1], "Iy": iy[1], "It": it[1],
+               "den": den[1]}
 
 
 def _match_den(expr, ix, iy) -> Optional[str]:
@@ -373,25 +374,29 @@ def lower_hs_loops(prog: Program) -> None:
         top_assigned = _assigned(before)
         counts = {n: top_assigned.count(n) for n in set(top_assigned)}
         invariant = {n for n in (set(prog.params) | set(top_assigned)) if n not in loop_assigned}
-        m = _match_hs_body(final, loop_assigned, invariant)
-        if m is None:
-            continue
-        # den must be defined once before the loop as (alpha2 + Ix*Ix) + Iy*Iy
-        if counts.get(m["den"], 0) != 1 or any(counts.get(m[k], 0) > 1 for k in ("Ix", "Iy", "It")):
-            continue
-        pre = _symbolic(before, {})
-        if pre is None or m["den"] not in pre:
-            continue
-        # substitute copies: the den expression refers to Ix, Iy by their own names
-        den_expr = _resolve_names(before, m["den"], {m["Ix"], m["Iy"]})
-        alpha2 = _match_den(den_expr, m["Ix"], m["Iy"]) if den_expr is not None else None
-        if alpha2 is None:
-            continue
-        # every other name the loop assigns must be dead after it
         live_after = _names_read_after(body[i + 1:])
-        if any(n in live_after for n in loop_assigned if n not in (m["U"], m["V"])):
+        pre = _symbolic(before, {})
+        chosen = None
+        for m in _match_hs_body(final, loop_assigned, invariant):
+            # den must be defined once before the loop as (alpha2 + Ix*Ix) + Iy*Iy
+            if counts.get(m["den"], 0) != 1 or any(counts.get(m[k], 0) > 1 for k in ("Ix", "Iy", "It")):
+                continue
+            if pre is None or m["den"] not in pre:
+                continue
+            # the den expression refers to Ix, Iy by their own names
+            den_expr = _resolve_names(before, m["den"], {m["Ix"], m["Iy"]})
+            alpha2 = _match_den(den_expr, m["Ix"], m["Iy"])
+            if alpha2 is None:
+                continue
+            # every other name the loop assigns must be dead after it
+            if any(n in live_after for n in loop_assigned if n not in (m["U"], m["V"])):
+                continue
+            m["alpha2"] = alpha2
+            chosen = m
+            break
+        if chosen is None:
             continue
-        m["alpha2"] = alpha2
+        m = chosen
         body[i] = Stmt("HSSweeps", info=m, ub=s.ub, body=s.body)
 
 

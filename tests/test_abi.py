@@ -1,0 +1,105 @@
+"""The C-ABI library: it loads, exports exactly what include/hsflow.h declares, and its
+argument checks return the documented status before any device work (these calls
+touch no GPU, so they run on CPU)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from hindemith_b200 import _lib as L
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = []
+    for h in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if h.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", h)).read()
+            names += re.findall(r"^HS_API\s+[\w\s\*]*?\b(hs_\w+)\s*\(", src, flags=re.M)
+    return names
+
+
+def test_library_loads_and_exports_every_declared_symbol():
+    lib = L.lib()
+    names = declared_functions()
+    assert len(names) >= 13
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/ but not exported"
+        assert n in L.SIGNATURES, f"{n} has no ctypes signature in _lib.py"
+
+
+def test_status_strings():
+    for code in range(8):
+        s = L.status_string(code)
+        assert s and "unknown" not in s
+    assert "unknown" in L.status_string(99)
+
+
+def test_version():
+    assert L.lib().hs_version() >= 100
+
+
+def fake_ptr(offset=0):
+    # never dereferenced: every call below fails its argument check first
+    return ctypes.c_void_p(0x100000 + offset)
+
+
+def test_argument_checks_before_launch():
+    lib = L.lib()
+    P = fake_ptr()
+    w = np.ones(3, np.float32)
+    o = np.zeros(3, np.int32)
+    wp, op_ = w.ctypes.data_as(L._fp), o.ctypes.data_as(L._ip)
+    # bad geometry
+    assert lib.hs_stencil2d(wp, op_, op_, 3, P, fake_ptr(256), 0, 4, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_stencil2d(wp, op_, op_, 3, P, fake_ptr(256), 4, 5, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_stencil2d(wp, op_, op_, 3, P, fake_ptr(256), 4, 5, 6, None) == L.HS_ERR_ALIGNMENT
+    # tap count
+    assert lib.hs_stencil2d(wp, op_, op_, 0, P, fake_ptr(256), 4, 4, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_stencil2d(wp, op_, op_, 65, P, fake_ptr(256), 4, 4, 4, None) == L.HS_ERR_INVALID_ARG
+    # aliasing and alignment
+    assert lib.hs_stencil2d(wp, op_, op_, 3, P, P, 4, 4, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_stencil2d(wp, op_, op_, 3, fake_ptr(4), fake_ptr(256), 4, 4, 4, None) == L.HS_ERR_ALIGNMENT
+    assert b"16-byte" in lib.hs_last_error()
+    # bad op code
+    assert lib.hs_array2d_op(7, P, P, P, 4, 4, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_array2d_op(0, None, P, P, 4, 4, 4, None) == L.HS_ERR_INVALID_ARG
+
+
+def test_sweep_argument_checks():
+    lib = L.lib()
+    P = fake_ptr()
+    cfg = L.make_config()
+    H, W, ld = 8, 8, 8
+    need = lib.hs_sweeps_workspace_bytes(H, W, ld)
+    assert need == 2 * 256  # two 8x8 float planes, each rounded to 256 bytes
+    assert lib.hs_forward_workspace_bytes(H, W, ld) == 5 * 256
+    # iters < 0
+    st = lib.hs_sweeps(P, P, P, H, W, ld, 1.0, -1, P, P, P, need, ctypes.byref(cfg), None)
+    assert st == L.HS_ERR_INVALID_ARG
+    # iters == 0 is a no-op that needs no workspace
+    st = lib.hs_sweeps(P, P, P, H, W, ld, 1.0, 0, P, P, None, 0, ctypes.byref(cfg), None)
+    assert st == L.HS_OK
+    # workspace too small
+    st = lib.hs_sweeps(P, P, P, H, W, ld, 1.0, 5, P, P, P, need - 1, ctypes.byref(cfg), None)
+    assert st == L.HS_ERR_WORKSPACE
+    # T out of range, reserved fields
+    bad = L.make_config(sweeps_per_pass=9)
+    st = lib.hs_sweeps(P, P, P, H, W, ld, 1.0, 5, P, P, P, need, ctypes.byref(bad), None)
+    assert st == L.HS_ERR_INVALID_ARG
+    bad = L.make_config()
+    bad.reserved[1] = 3
+    st = lib.hs_forward(P, P, H, W, ld, 1.0, 5, P, P, P, 10 ** 6, ctypes.byref(bad), None)
+    assert st == L.HS_ERR_INVALID_ARG
+    st = lib.hs_forward(P, P, H, W, ld, 1.0, 5, P, P, P, 10, ctypes.byref(cfg), None)
+    assert st == L.HS_ERR_WORKSPACE
+
+
+def test_hs_error_raises_with_detail():
+    with pytest.raises(L.HSError) as ei:
+        L.check(L.lib().hs_array2d_op(9, fake_ptr(), fake_ptr(), fake_ptr(), 4, 4, 4, None), "hs_array2d_op")
+    assert ei.value.status == L.HS_ERR_INVALID_ARG
+    assert "op=9" in str(ei.value)

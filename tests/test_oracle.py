@@ -1,0 +1,116 @@
+"""The oracle is pinned before it is trusted: NumPy and C restatements against the
+golden fixtures produced by the reference's own hlib.py (tests/golden/make_golden.py),
+bit for bit, plus properties of the FP64 path."""
+import numpy as np
+import pytest
+
+from conftest import assert_bitexact, golden, golden_files
+from oracle import hs_oracle as O
+
+
+@pytest.mark.parametrize("path", golden_files("stencil_*.npz"))
+def test_stencil_golden(path):
+    d = np.load(path)
+    for i, (H, W) in enumerate(d["shapes"]):
+        x, ref = d[f"x{i}"], d[f"out{i}"]
+        assert_bitexact(O.stencil2d(d["weights"], d["offx"], d["offy"], x), ref, f"numpy {path} {i}")
+        assert_bitexact(O.c_stencil2d(d["weights"], d["offx"], d["offy"], x), ref, f"C {path} {i}")
+
+
+@pytest.mark.parametrize("path", golden_files("hs_*.npz"))
+def test_hs_program_golden(path):
+    d = np.load(path)
+    Ix, Iy, It = O.hs_derivs(d["I0"], d["I1"])
+    for a, name in ((Ix, "Ix"), (Iy, "Iy"), (It, "It")):
+        assert_bitexact(a, d[name], name)
+    cIx, cIy, cIt = O.c_hs_derivs(d["I0"], d["I1"])
+    for a, name in ((cIx, "Ix"), (cIy, "Iy"), (cIt, "It")):
+        assert_bitexact(a, d[name], "C " + name)
+    z = np.zeros_like(d["I0"])
+    n = int(d["sweeps"])
+    u, v = O.hs_sweeps(Ix, Iy, It, d["alpha2"], n, z, z)
+    assert_bitexact(u, d["u"], "u")
+    assert_bitexact(v, d["v"], "v")
+    cu, cv = O.c_hs_sweeps(Ix, Iy, It, float(d["alpha2"]), n, z, z)
+    assert_bitexact(cu, d["u"], "C u")
+    assert_bitexact(cv, d["v"], "C v")
+
+
+def test_warp_golden():
+    """hlib.warp_img2d agrees with WarpImg2D.cpp for integer offsets except on the last
+    row/column when that axis's offset is 0: the device template demands x+dx+1 < W
+    (it always reads the 2x2 footprint) and keeps the source pixel there, while
+    warp_img2d steps by sign(0) = 0.  The oracle follows the device template."""
+    for name in ("warp_int.npz", "warp_zero.npz"):
+        d = golden(name)
+        src, ox, oy, ref = d["src"], d["ox"], d["oy"], d["out"]
+        H, W = src.shape
+        Y, X = np.mgrid[0:H, 0:W]
+        device_rule = ((ox == 0) & (oy != 0) & (X == W - 1)) | ((oy == 0) & (ox != 0) & (Y == H - 1))
+        for fn in (O.warp, O.c_warp):
+            out = fn(src, ox, oy)
+            np.testing.assert_array_equal(out[~device_rule], ref[~device_rule])
+            np.testing.assert_array_equal(out[device_rule], src[device_rule])
+
+
+def test_warp_fractional_numpy_vs_c():
+    rng = np.random.default_rng(3)
+    src = rng.random((23, 29), dtype=np.float32)
+    ox = (rng.random((23, 29)) * 8 - 4).astype(np.float32)
+    oy = (rng.random((23, 29)) * 8 - 4).astype(np.float32)
+    assert_bitexact(O.warp(src, ox, oy), O.c_warp(src, ox, oy), "warp")
+
+
+def test_fp64_oracle_close_to_fp32():
+    from hindemith_b200 import synthetic
+
+    I0, I1, _, _ = synthetic.make_pair(64, 80, seed=1000)
+    u32, v32 = O.c_hs_forward(I0, I1, 1.0, 100, np.float32)
+    u64, v64 = O.c_hs_forward(I0, I1, 1.0, 100, np.float64)
+    assert np.abs(u32 - u64).max() < 1e-5
+    assert np.abs(v32 - v64).max() < 1e-5
+    un, vn = O.hs_forward(I0, I1, 1.0, 100, np.float64)
+    np.testing.assert_allclose(un, u64, rtol=0, atol=1e-12)
+
+
+def test_numpy_and_c_forward_agree_bitwise():
+    from hindemith_b200 import synthetic
+
+    I0, I1, _, _ = synthetic.make_pair(37, 53, seed=1001)
+    a = O.hs_forward(I0, I1, 0.7, 25, np.float32)
+    b = O.c_hs_forward(I0, I1, 0.7, 25, np.float32)
+    assert_bitexact(a[0], b[0], "u")
+    assert_bitexact(a[1], b[1], "v")
+
+
+def test_known_answers():
+    # a constant image has zero derivatives, so the flow stays exactly 0
+    c = np.full((9, 11), 0.37, dtype=np.float32)
+    u, v = O.c_hs_forward(c, c, 1.0, 50)
+    assert not u.any() and not v.any()
+    # a horizontal ramp translated by s: It/Ix = -s in the interior, and with a small
+    # alpha the interior flow approaches (s, 0)
+    H, W, s = 24, 40, 0.5
+    x = np.arange(W, dtype=np.float64)
+    I0 = np.tile(0.02 * x, (H, 1)).astype(np.float32)
+    I1 = np.tile(0.02 * (x - s), (H, 1)).astype(np.float32)
+    Ix, Iy, It = O.c_hs_derivs(I0, I1, np.float64)
+    mid = (slice(2, -2), slice(2, -2))
+    np.testing.assert_allclose(It[mid] / Ix[mid], -s, atol=1e-6)
+    u, v = O.c_hs_forward(I0, I1, 0.01, 2000, np.float64)
+    assert np.abs(u[8:-8, 8:-8] - s).max() < 1e-3
+    assert np.abs(v).max() < 1e-6
+
+
+def test_stencil_transpose_adjoint():
+    """<S x, y> = <x, S^T y> in FP64 for clamp-to-edge stencils."""
+    rng = np.random.default_rng(5)
+    for (H, W) in ((1, 1), (1, 6), (5, 1), (7, 9)):
+        x = rng.standard_normal((H, W))
+        y = rng.standard_normal((H, W))
+        for w, ox, oy in ((O.AVG_W, O.AVG_OFFX, O.AVG_OFFY), (O.DX_W, O.D_OFFX, O.D_OFFY)):
+            w = w.astype(np.float64)
+            Sx = O.c_stencil2d(w, ox, oy, x, np.float64)
+            STy = O.c_stencil2d_transpose(w, ox, oy, y)
+            assert abs((Sx * y).sum() - (x * STy).sum()) < 1e-12
+            np.testing.assert_allclose(STy, O.stencil2d_transpose(w, ox, oy, y), atol=1e-14)
