@@ -3,7 +3,8 @@
 For an image shape it times candidate (T, rows_per_segment) pairs with CUDA events on
 the device (a fixed number of sweeps over synthetic coefficient planes of that shape)
 and keeps the fastest.  Results are cached per (device name, H, W, ld, mode) in memory
-and, when HS_AUTOTUNE_CACHE names a file, in that JSON file.
+and, when HS_AUTOTUNE_CACHE names a file, in that JSON file.  HS_AUTOTUNE_LOG names a
+file that receives every candidate's timing as one JSON line per tuning.
 """
 from __future__ import annotations
 
@@ -103,6 +104,14 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
             results.append((ms, T, seg))
     results.sort()
     best = (results[0][1], results[0][2])
+    log = os.environ.get("HS_AUTOTUNE_LOG")
+    if log:
+        try:
+            with open(log, "a") as f:
+                f.write(json.dumps({"key": key, "sweeps": sweeps,
+                                    "ms": [[round(ms, 5), T, seg] for ms, T, seg in results]}) + "\n")
+        except OSError:
+            pass
     with _lock:
         _cache[key] = best
         _save_file()
