@@ -77,7 +77,10 @@ SIGNATURES = {
     "hs_sweeps": (_i, [_vp, _vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _vp, _sz, _cfgp, _vp]),
     "hs_forward_workspace_bytes": (_sz, [_i, _i, _i]),
     "hs_forward": (_i, [_vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _vp, _sz, _cfgp, _vp]),
+    "hs_forward_noalloc": (_i, [_vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _cfgp, _vp]),
 }
+
+HS_NOALLOC_SCRATCH_BYTES = 48 << 20
 
 
 def lib():

@@ -126,6 +126,31 @@ HS_API hs_status hs_forward(const float *I0, const float *I1, int H, int W, int 
                      int iters, float *u, float *v, void *workspace, size_t workspace_bytes,
                      const hs_config *cfg, void *stream);
 
+/* ---- allocation-free forward ------------------------------------------------- */
+
+/* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for
+ * planes of up to H * ld * 4 = 10,066,176 bytes (e.g. 1920x1080 with ld = 1920). */
+#define HS_NOALLOC_SCRATCH_BYTES (48u << 20)
+
+/* hs_forward without a caller-supplied workspace.  No counterpart in the reference: it
+ * serves callers that cannot allocate device memory -- a frame loop that must not call
+ * cudaMalloc/cudaFree (they can synchronise the device mid-stream), or a host binding
+ * that has no way to own and release a device buffer.  The caller still passes the
+ * inputs I0, I1 and the outputs u, v; the scratch is a static __device__ array of
+ * HS_NOALLOC_SCRATCH_BYTES inside this library, held by every GPU that loads the
+ * library until the process exits.  Nothing here allocates or frees memory.
+ *   - Sizes whose five scratch planes exceed HS_NOALLOC_SCRATCH_BYTES are rejected with
+ *     HS_ERR_WORKSPACE before any device work.
+ *   - The first call on a device looks up the scratch's device address (with that
+ *     device current); make that first call before any stream capture.
+ *   - All calls on a device share the one scratch array and it keeps the last call's
+ *     contents (each call initialises what it reads).  Calls that overlap on the GPU --
+ *     concurrent streams, or several host threads -- race on it; serialise them.
+ * Results are identical to hs_forward with the same arguments and config. */
+HS_API hs_status hs_forward_noalloc(const float *I0, const float *I1, int H, int W, int ld,
+                                    float alpha, int iters, float *u, float *v,
+                                    const hs_config *cfg, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
