@@ -31,19 +31,22 @@
 
 namespace hs {
 
-constexpr int kWarpCols = 64;      // columns per strip (2 per lane)
-constexpr int kPrefetch = 3;       // rows in flight per warp
-constexpr int kWarpsPerBlock = 4;  // independent warps per CTA
-constexpr int kPlanes = 6;         // ring planes: u, v, Ix, Iy, It, aux
+constexpr int kWarpCols = 64;                 // columns per strip (2 per lane)
+constexpr int kPrefetch = 3;                  // rows in flight per warp
+constexpr int kRawSlots = kPrefetch + 1;      // raw-row ring depth (a power of two)
+constexpr int kRawPlanes = 5;                 // u, v, Ix, Iy, It as copied from HBM
+constexpr int kWarpsPerBlock = 4;             // independent warps per CTA
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int T>
 struct Geo {
-    static constexpr int halo = (T + 1) & ~1;                 // even, so lanes load float2
-    static constexpr int strip = kWarpCols - 2 * halo;        // output columns per strip
-    static constexpr int slots = T + 1 + kPrefetch;           // ring rows per warp
-    static constexpr int ring_floats = slots * kPlanes * kWarpCols;
-    static constexpr int smem_bytes = kWarpsPerBlock * ring_floats * (int)sizeof(float);
+    static constexpr int halo = (T + 1) & ~1;                  // even, so lanes load float2
+    static constexpr int strip = kWarpCols - 2 * halo;         // output columns per strip
+    static constexpr int coef_slots = T + 1;                   // rows k-T .. k
+    static constexpr int raw_floats = kRawSlots * kRawPlanes * kWarpCols;
+    static constexpr int coef_floats = coef_slots * 2 * 32 * 4;  // [slot][column][lane] float4
+    static constexpr int warp_floats = raw_floats + coef_floats;
+    static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
 };
 
 struct SweepParams {
@@ -76,12 +79,82 @@ __device__ __forceinline__ void griddep_launch_dependents() {
 }
 __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
 
-// Issue the async copy of input row `row` (clamped into the image) into ring slot `slot`.
-__device__ __forceinline__ void issue_row(float *ring, int slot, int row, const SweepParams &p,
-                                          int lc, int lane) {
+// Hardware reciprocal approximation (PTX rcp.approx, about 1 ulp) for the fast form.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+
+// Sliding three-row window of one stage, one plane, one column.
+//   fast : with Y(k) = we*c(k) + wc*h(k) (h = left + right), the average of row n-1 is
+//          Y(n-2) + we*h(n-1) + Y(n).  Z = Y(n-2) + we*h(n-1) and Y1 = Y(n-1) are kept,
+//          so a row costs 5 operations and 2 registers.
+//   exact: A0 = next row's accumulator holding its up taps (taken from row n-1),
+//          A1 = row n-1's accumulator holding its up and mid taps, l1/c1/r1 = row n-1
+//          (read only for the bottom clamp)
+template <bool FAST>
+struct Win;
+template <>
+struct Win<true> {
+    float Z, Y1;
+};
+template <>
+struct Win<false> {
+    float A0, A1, l1, c1, r1;
+};
+
+// Row n arrives (values l, c, r at this column); returns the average of row n-1 and
+// advances the window.  EDGE: the row may be row 0 (top clamp) or past the bottom
+// (replaced by row H-1, the bottom clamp).
+template <bool EDGE>
+__device__ __forceinline__ float win_step(Win<true> &w, float l, float c, float r, int n, int H,
+                                          float we, float wc) {
+    const float hn = l + r;
+    float yn = fmaf(we, c, wc * hn);
+    if (EDGE && n >= H) yn = w.Y1;  // the row below H-1 is row H-1
+    const float out = w.Z + yn;
+    w.Z = fmaf(we, hn, (EDGE && n == 0) ? yn : w.Y1);  // row 0's up row is row 0
+    w.Y1 = yn;
+    return out;
+}
+
+template <bool EDGE>
+__device__ __forceinline__ float win_step(Win<false> &w, float l, float c, float r, int n, int H,
+                                          float we, float wc) {
+    if (EDGE && n >= H) { l = w.l1; c = w.c1; r = w.r1; }
+    // taps in row-major order: (-1,-1) (0,-1) (1,-1) | (-1,0) (1,0) | (-1,1) (0,1) (1,1)
+    float o = w.A1;                              // row n-1: up and mid taps done
+    o = __fadd_rn(o, __fmul_rn(wc, l));          // its dn taps come from row n
+    o = __fadd_rn(o, __fmul_rn(we, c));
+    o = __fadd_rn(o, __fmul_rn(wc, r));
+    float up = __fadd_rn(0.0f, __fmul_rn(wc, l));  // row n+1's up taps come from row n
+    up = __fadd_rn(up, __fmul_rn(we, c));
+    up = __fadd_rn(up, __fmul_rn(wc, r));
+    float am = (EDGE && n == 0) ? up : w.A0;     // row 0's up taps are its own (clamp)
+    am = __fadd_rn(am, __fmul_rn(we, l));        // row n's mid taps
+    am = __fadd_rn(am, __fmul_rn(we, r));
+    w.A0 = up;
+    w.A1 = am;
+    if (EDGE) { w.l1 = l; w.c1 = c; w.r1 = r; }
+    return o;
+}
+
+// Per-warp context of one work item.
+struct Item {
+    float *raw;    // [kRawSlots][kRawPlanes][64] floats
+    float4 *coef;  // [T+1][2][32]
+    int lane, lc;
+    bool a_first, a_last, b_last, st_a, st_b;
+    int xa, y_start, y_end;
+};
+
+__device__ __forceinline__ void issue_row(const Item &it, int slot, int row, const SweepParams &p) {
     row = min(max(row, 0), p.H - 1);
-    const size_t off = (size_t)row * p.ld + lc;
-    float *base = ring + slot * (kPlanes * kWarpCols) + 2 * lane;
+    const size_t off = (size_t)row * p.ld + it.lc;
+    float *base = it.raw + slot * (kRawPlanes * kWarpCols) + 2 * it.lane;
     cp_async8(base + 0 * kWarpCols, p.u_in + off);
     cp_async8(base + 1 * kWarpCols, p.v_in + off);
     cp_async8(base + 2 * kWarpCols, p.Ix + off);
@@ -90,16 +163,149 @@ __device__ __forceinline__ void issue_row(float *ring, int slot, int row, const 
     cp_async_commit();
 }
 
-__device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+// One streaming step: row k arrives at stage 0, stage s emits sweep s+1 of row k-s-1.
+template <int T, bool FAST, bool XEDGE, bool EDGE>
+__device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it, Win<FAST> (&w)[T][2][2],
+                                            int k, int rslot, int cslot) {
+    // prefetch row k + kPrefetch into the slot row k-1 used, then wait for row k
+    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), k + kPrefetch, p);
+    cp_async_wait<kPrefetch>();
+
+    // stage 0: unpack row k; pack its coefficients with the denominator term
+    const float *raw = it.raw + rslot * (kRawPlanes * kWarpCols) + 2 * it.lane;
+    const float2 u2 = lds2(raw), v2 = lds2(raw + kWarpCols);
+    {
+        const float2 ix = lds2(raw + 2 * kWarpCols), iy = lds2(raw + 3 * kWarpCols);
+        const float2 t2 = lds2(raw + 4 * kWarpCols);
+        float ax, ay;
+        if constexpr (FAST) {
+            ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, p.alpha2)));
+            ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, p.alpha2)));
+        } else {
+            ax = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.x, ix.x)), __fmul_rn(iy.x, iy.x));
+            ay = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.y, ix.y)), __fmul_rn(iy.y, iy.y));
+        }
+        float4 *cs = it.coef + cslot * 64 + it.lane;
+        cs[0] = make_float4(ix.x, iy.x, t2.x, ax);
+        cs[32] = make_float4(ix.y, iy.y, t2.y, ay);
+    }
+    float cu[2][2] = {{u2.x, u2.y}, {v2.x, v2.y}};  // [plane][column]
+
+#pragma unroll
+    for (int s = 0; s < T; ++s) {
+        const int n = k - s;  // arriving row (input of sweep s+1)
+        float ub[2][2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float ca = cu[q][0], cb = cu[q][1];
+            const float fromL = __shfl_up_sync(kFull, cb, 1);
+            const float fromR = __shfl_down_sync(kFull, ca, 1);
+            float la = fromL, ra = cb, rb = fromR;
+            if constexpr (XEDGE) {
+                la = it.a_first ? ca : la;
+                ra = it.a_last ? ca : ra;
+                rb = it.b_last ? cb : rb;
+            }
+            ub[q][0] = win_step<EDGE>(w[s][q][0], la, ca, ra, n, p.H, p.we, p.wc);
+            ub[q][1] = win_step<EDGE>(w[s][q][1], ca, cb, rb, n, p.H, p.we, p.wc);
+        }
+        // pointwise update of row n-1 with its coefficients
+        int rs = cslot - (s + 1);
+        if (rs < 0) rs += Geo<T>::coef_slots;
+        const float4 *cr = it.coef + rs * 64 + it.lane;
+        const float4 C[2] = {cr[0], cr[32]};
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const float ubar = ub[0][j], vbar = ub[1][j];
+            if constexpr (FAST) {
+                const float r = fmaf(C[j].x, ubar, fmaf(C[j].y, vbar, C[j].z));
+                const float t = r * C[j].w;
+                cu[0][j] = fmaf(-C[j].x, t, ubar);
+                cu[1][j] = fmaf(-C[j].y, t, vbar);
+            } else {
+                float r = __fadd_rn(__fmul_rn(C[j].x, ubar), __fmul_rn(C[j].y, vbar));
+                r = __fadd_rn(r, C[j].z);
+                const float t = __fdiv_rn(r, C[j].w);
+                cu[0][j] = __fsub_rn(ubar, __fmul_rn(C[j].x, t));
+                cu[1][j] = __fsub_rn(vbar, __fmul_rn(C[j].y, t));
+            }
+        }
+    }
+
+    // store sweep T of row k - T
+    const int r = k - T;
+    if (r >= it.y_start && r < it.y_end) {
+        const size_t off = (size_t)r * p.ld + it.xa;
+        if (it.st_a && it.st_b) {
+            *reinterpret_cast<float2 *>(p.u_out + off) = make_float2(cu[0][0], cu[0][1]);
+            *reinterpret_cast<float2 *>(p.v_out + off) = make_float2(cu[1][0], cu[1][1]);
+        } else if (it.st_a) {
+            p.u_out[off] = cu[0][0];
+            p.v_out[off] = cu[1][0];
+        }
+    }
+}
+
+template <int T, bool FAST, bool XEDGE>
+__device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it) {
+    const int k0 = max(0, it.y_start - T);
+    const int k_end = it.y_end - 1 + T;
+    Win<FAST> w[T][2][2];
+#pragma unroll
+    for (int s = 0; s < T; ++s)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) w[s][q][j] = Win<FAST>{};
+
+#pragma unroll
+    for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, p);
+
+    // Steps in [klo, khi] have no stage at row 0 or past row H-2: no clamp logic.
+    const int klo = max(k0, T);
+    const int khi = min(k_end, p.H - 2);
+    int k = k0, rslot = 0, cslot = 0;
+    auto advance = [&]() {
+        ++k;
+        rslot = (rslot + 1) & (kRawSlots - 1);
+        cslot = (cslot + 1 == Geo<T>::coef_slots) ? 0 : cslot + 1;
+    };
+    if (klo + 1 <= khi) {
+        for (; k < klo; advance()) stream_step<T, FAST, XEDGE, true>(p, it, w, k, rslot, cslot);
+        while (k + 1 <= khi) {
+            stream_step<T, FAST, XEDGE, false>(p, it, w, k, rslot, cslot);
+            advance();
+            stream_step<T, FAST, XEDGE, false>(p, it, w, k, rslot, cslot);
+            advance();
+        }
+        // Here k <= H-1, so row H-1 reaches every stage in the tail loop below.  The
+        // bottom-clamp values are written and read only there; dropping the head loop's
+        // copies keeps them out of the main loop's live registers.
+        if constexpr (!FAST) {
+#pragma unroll
+            for (int s = 0; s < T; ++s)
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int j = 0; j < 2; ++j) w[s][q][j].l1 = w[s][q][j].c1 = w[s][q][j].r1 = 0.f;
+        }
+    }
+    for (; k <= k_end; advance()) stream_step<T, FAST, XEDGE, true>(p, it, w, k, rslot, cslot);
+    cp_async_wait<0>();
+}
+
+// Resident CTAs per SM the register budget is sized for (shared memory allows it too).
+// (Measured: capping registers for more CTAs costs more ILP than it gains.)
+constexpr int min_blocks(int T) { return T <= 4 ? 4 : (T <= 6 ? 3 : 2); }
 
 template <int T, bool FAST>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : 2))
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks(T))
     hs_stream_kernel(const SweepParams p) {
     using G = Geo<T>;
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float *ring = reinterpret_cast<float *>(smem4) + warp * G::ring_floats;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * G::warp_floats;
 
     griddep_launch_dependents();
     griddep_wait();
@@ -109,152 +315,27 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : 2))
     const int strip = item % p.nstrips;
     const int seg = item / p.nstrips;
     const int x0 = strip * G::strip - G::halo;
-    const int xa = x0 + 2 * lane, xb = xa + 1;
+    Item it;
+    it.raw = wbase;
+    it.coef = reinterpret_cast<float4 *>(wbase + G::raw_floats);
+    it.lane = lane;
+    it.xa = x0 + 2 * lane;
+    const int xb = it.xa + 1;
     // Column pair each lane loads: its own when it starts inside the image (xa is even
     // and ld is a multiple of 4, so xa + 1 < ld), any in-bounds pair otherwise -- columns
     // outside the image never feed a stored pixel.
-    const int lc = (xa >= 0 && xa < p.W) ? xa : 0;
-    const bool a_first = (xa == 0), a_last = (xa == p.W - 1), b_last = (xb == p.W - 1);
+    it.lc = (it.xa >= 0 && it.xa < p.W) ? it.xa : 0;
+    it.a_first = (it.xa == 0);
+    it.a_last = (it.xa == p.W - 1);
+    it.b_last = (xb == p.W - 1);
     const int vlo = strip * G::strip, vhi = min(vlo + G::strip, p.W);
-    const bool st_a = (xa >= vlo && xa < vhi), st_b = (xb >= vlo && xb < vhi);
-    const int y_start = seg * p.seg_rows;
-    const int y_end = min(p.H, y_start + p.seg_rows);
-    const int k0 = max(0, y_start - T);
-    const int k_end = y_end - 1 + T;
-    const float we = p.we, wc = p.wc;
-
-    // Per-stage window state, [stage][plane u/v][column a/b].
-    // fast:  cm = centre of the mid row, hm = its horizontal pair sum,
-    //        E = c(up) + h(mid) (edge partial), C = h(up) (corner partial).
-    // exact: A0 = accumulator of the next row holding its up taps, A1 = accumulator of
-    //        the mid row holding its up and mid taps, lm/cm/rm = the mid row's values.
-    float s0[T][2][2], s1[T][2][2], s2[T][2][2], s3[T][2][2], s4[T][2][2];
-#pragma unroll
-    for (int s = 0; s < T; ++s)
-#pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) s0[s][q][j] = s1[s][q][j] = s2[s][q][j] = s3[s][q][j] = s4[s][q][j] = 0.f;
-
-#pragma unroll
-    for (int i = 0; i < kPrefetch; ++i) issue_row(ring, i, k0 + i, p, lc, lane);
-
-    int kslot = 0;
-    for (int k = k0; k <= k_end; ++k) {
-        int pslot = kslot + kPrefetch;
-        if (pslot >= G::slots) pslot -= G::slots;
-        issue_row(ring, pslot, k + kPrefetch, p, lc, lane);
-        cp_async_wait<kPrefetch>();
-
-        // ---- stage 0: row k arrives; derive the per-pixel denominator term.
-        float *sl = ring + kslot * (kPlanes * kWarpCols) + 2 * lane;
-        const float2 u2 = lds2(sl), v2 = lds2(sl + kWarpCols);
-        {
-            const float2 ix = lds2(sl + 2 * kWarpCols), iy = lds2(sl + 3 * kWarpCols);
-            float2 aux;
-            if constexpr (FAST) {
-                aux.x = 1.0f / fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, p.alpha2));
-                aux.y = 1.0f / fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, p.alpha2));
-            } else {
-                aux.x = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.x, ix.x)), __fmul_rn(iy.x, iy.x));
-                aux.y = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.y, ix.y)), __fmul_rn(iy.y, iy.y));
-            }
-            *reinterpret_cast<float2 *>(sl + 5 * kWarpCols) = aux;
-        }
-        float cu[2][2] = {{u2.x, u2.y}, {v2.x, v2.y}};  // [plane][column]
-
-        // ---- stages 1..T
-#pragma unroll
-        for (int s = 0; s < T; ++s) {
-            const int n = k - s;  // arriving row (input of sweep s+1)
-            float ub[2][2];       // averages of output row n-1, [plane][column]
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                const float ca = cu[q][0], cb = cu[q][1];
-                const float fromL = __shfl_up_sync(kFull, cb, 1);
-                const float fromR = __shfl_down_sync(kFull, ca, 1);
-                const float la = a_first ? ca : fromL;
-                const float ra = a_last ? ca : cb;
-                const float lb = ca;
-                const float rb = b_last ? cb : fromR;
-                const float L[2] = {la, lb}, Cc[2] = {ca, cb}, R[2] = {ra, rb};
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    if constexpr (FAST) {
-                        float cn = Cc[j], hn = L[j] + R[j];
-                        if (n >= p.H) { cn = s0[s][q][j]; hn = s1[s][q][j]; }
-                        ub[q][j] = fmaf(s2[s][q][j] + cn, we, (s3[s][q][j] + hn) * wc);
-                        if (n == 0) { s2[s][q][j] = cn + hn; s3[s][q][j] = hn; }
-                        else { s2[s][q][j] = s0[s][q][j] + hn; s3[s][q][j] = s1[s][q][j]; }
-                        s0[s][q][j] = cn;
-                        s1[s][q][j] = hn;
-                    } else {
-                        float l = L[j], c = Cc[j], r = R[j];
-                        if (n >= p.H) { l = s2[s][q][j]; c = s3[s][q][j]; r = s4[s][q][j]; }
-                        // finish the mid row with the dn taps (-1,1) (0,1) (1,1)
-                        float o = s1[s][q][j];
-                        o = __fadd_rn(o, __fmul_rn(wc, l));
-                        o = __fadd_rn(o, __fmul_rn(we, c));
-                        o = __fadd_rn(o, __fmul_rn(wc, r));
-                        ub[q][j] = o;
-                        // up taps (-1,-1) (0,-1) (1,-1) of the next row come from this row
-                        float up = __fadd_rn(0.0f, __fmul_rn(wc, l));
-                        up = __fadd_rn(up, __fmul_rn(we, c));
-                        up = __fadd_rn(up, __fmul_rn(wc, r));
-                        // this row becomes the mid row: its own mid taps (-1,0) (1,0); row 0
-                        // takes its up taps from itself (clamp)
-                        float am = (n == 0) ? up : s0[s][q][j];
-                        am = __fadd_rn(am, __fmul_rn(we, l));
-                        am = __fadd_rn(am, __fmul_rn(we, r));
-                        s0[s][q][j] = up;
-                        s1[s][q][j] = am;
-                        s2[s][q][j] = l;
-                        s3[s][q][j] = c;
-                        s4[s][q][j] = r;
-                    }
-                }
-            }
-            // pointwise update of row n-1 with its coefficients from the ring
-            int rs = kslot - (s + 1);
-            if (rs < 0) rs += G::slots;
-            const float *cr = ring + rs * (kPlanes * kWarpCols) + 2 * lane;
-            const float2 ix2 = lds2(cr + 2 * kWarpCols), iy2 = lds2(cr + 3 * kWarpCols);
-            const float2 it2 = lds2(cr + 4 * kWarpCols), ax2 = lds2(cr + 5 * kWarpCols);
-            const float IX[2] = {ix2.x, ix2.y}, IY[2] = {iy2.x, iy2.y};
-            const float IT[2] = {it2.x, it2.y}, AX[2] = {ax2.x, ax2.y};
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const float ubar = ub[0][j], vbar = ub[1][j];
-                if constexpr (FAST) {
-                    const float r = fmaf(IX[j], ubar, fmaf(IY[j], vbar, IT[j]));
-                    const float t = r * AX[j];
-                    cu[0][j] = fmaf(-IX[j], t, ubar);
-                    cu[1][j] = fmaf(-IY[j], t, vbar);
-                } else {
-                    float r = __fadd_rn(__fmul_rn(IX[j], ubar), __fmul_rn(IY[j], vbar));
-                    r = __fadd_rn(r, IT[j]);
-                    const float t = __fdiv_rn(r, AX[j]);
-                    cu[0][j] = __fsub_rn(ubar, __fmul_rn(IX[j], t));
-                    cu[1][j] = __fsub_rn(vbar, __fmul_rn(IY[j], t));
-                }
-            }
-        }
-
-        // ---- store sweep T of row k - T
-        const int r = k - T;
-        if (r >= y_start && r < y_end) {
-            const size_t off = (size_t)r * p.ld + xa;
-            if (st_a && st_b) {
-                *reinterpret_cast<float2 *>(p.u_out + off) = make_float2(cu[0][0], cu[0][1]);
-                *reinterpret_cast<float2 *>(p.v_out + off) = make_float2(cu[1][0], cu[1][1]);
-            } else if (st_a) {
-                p.u_out[off] = cu[0][0];
-                p.v_out[off] = cu[1][0];
-            }
-        }
-        kslot = (kslot + 1 == G::slots) ? 0 : kslot + 1;
-    }
-    cp_async_wait<0>();
+    it.st_a = (it.xa >= vlo && it.xa < vhi);
+    it.st_b = (xb >= vlo && xb < vhi);
+    it.y_start = seg * p.seg_rows;
+    it.y_end = min(p.H, it.y_start + p.seg_rows);
+    // only strips reaching an image side need the horizontal clamp selects
+    if (x0 <= 0 || x0 + kWarpCols >= p.W) stream_item<T, FAST, true>(p, it);
+    else stream_item<T, FAST, false>(p, it);
 }
 
 // ------------------------------------------------------------------ host side
