@@ -51,6 +51,15 @@ class hs_config(ctypes.Structure):
     ]
 
 
+class hs_pair_desc(ctypes.Structure):
+    _fields_ = [("I0", ctypes.c_void_p), ("I1", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("v", ctypes.c_void_p), ("H", ctypes.c_int), ("W", ctypes.c_int),
+                ("ld", ctypes.c_int), ("alpha", ctypes.c_float), ("iters", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
+HS_MAX_BATCH = 128
+
 _lib = None
 _lock = threading.Lock()
 
@@ -61,6 +70,7 @@ _sz = ctypes.c_size_t
 _ip = ctypes.POINTER(ctypes.c_int)
 _fp = ctypes.POINTER(ctypes.c_float)
 _cfgp = ctypes.POINTER(hs_config)
+_pdp = ctypes.POINTER(hs_pair_desc)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -78,6 +88,8 @@ SIGNATURES = {
     "hs_forward_workspace_bytes": (_sz, [_i, _i, _i]),
     "hs_forward": (_i, [_vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _vp, _sz, _cfgp, _vp]),
     "hs_forward_noalloc": (_i, [_vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _cfgp, _vp]),
+    "hs_forward_batched_workspace_bytes": (_sz, [_pdp, _i, _cfgp]),
+    "hs_forward_batched": (_i, [_pdp, _i, _vp, _sz, _cfgp, _vp, _vp]),
 }
 
 HS_NOALLOC_SCRATCH_BYTES = 48 << 20

@@ -1,0 +1,461 @@
+// hs_batch.cu -- many Horn-Schunck pairs of uneven size in one persistent launch.
+//
+// Work list.  Every (pass, pair, segment, strip) tile of every pair's full T-sweep passes
+// is one work item.  Items are numbered pass-major: all of pass 0 (pair by pair, each
+// pair's tiles segment-major), then pass 1, ...; pairs are sorted by pass count, largest
+// first, so the pairs still active in pass p are a prefix of that order.  Warps take items
+// from a global atomic counter; a warp runs its item with the streaming sweep of
+// hs_stream.cuh and then publishes "tile done through pass p".
+//
+// Dependencies.  A tile's pass p reads rows and columns of pass p-1 reaching at most
+// one tile beyond its own in each direction (the halo is at most T rows and columns, a
+// segment is at least T rows and a strip at least 48 columns), and overwrites the buffer
+// those pass p-1 tiles read.  So pass p of tile (g, s) waits until its 3x3 neighbour
+// tiles have completed pass p-1.  Every tile an item waits on has a smaller item number,
+// so it was taken earlier by a running warp that waits only on smaller numbers still:
+// the waits always end.  Each wait is nevertheless bounded; a wait that gives up records
+// HS_ERR_TIMEOUT in the device status word and raises an abort flag on which every warp
+// stops.  Completion is published with a release store after the tile's writes and the
+// waits use acquire loads; rows are copied with cp.async.cg (L2), so no stale L1 line
+// is read.
+//
+// A pair whose sweep count is not a multiple of T finishes with one more, shorter pass
+// launched per pair after the persistent kernel.
+#include <algorithm>
+#include <mutex>
+#include <numeric>
+#include <vector>
+
+#include "hs_stream.cuh"
+
+namespace hs {
+
+constexpr int kMaxBatch = HS_MAX_BATCH;
+constexpr int kHeaderBytes = 256;                 // queue counter, status, abort flag
+constexpr unsigned long long kWaitPolls = 1ull << 22;  // bounded wait (seconds, at most)
+
+struct BatchPair {
+    const float *Ix, *Iy, *It;
+    float *U[2], *V[2];  // [0] = caller's output, [1] = scratch
+    unsigned *progress;  // per tile: passes completed
+    int H, W, ld;
+    float alpha2;
+    int passes;  // full T-sweep passes in the persistent kernel
+    int start;   // buffer the first pass reads
+    int nstrips, seg_rows, items;
+};
+
+struct BatchParams {
+    BatchPair pair[kMaxBatch];  // sorted by `passes`, descending
+    int item_prefix[kMaxBatch + 1];
+    // pass groups: passes [g_p0, g_p1) have the first g_active pairs active
+    int g_p0[kMaxBatch], g_p1[kMaxBatch], g_active[kMaxBatch], g_first[kMaxBatch];
+    int ngroups, npairs, total_items;
+    float we, wc;
+    unsigned *queue;
+    int *status;
+    unsigned *abort_flag;
+};
+
+struct DerivParams {
+    const float *I0[kMaxBatch], *I1[kMaxBatch];
+    float *Ix[kMaxBatch], *Iy[kMaxBatch], *It[kMaxBatch];
+    float *U0[kMaxBatch], *V0[kMaxBatch];  // initial-state buffers, zeroed here
+    int H[kMaxBatch], W[kMaxBatch], ld[kMaxBatch];
+    int npairs;
+};
+
+// Derivatives of every pair and u = v = 0 in the buffer each pair's first pass reads.
+__global__ void __launch_bounds__(256) batch_derivs_kernel(const __grid_constant__ DerivParams dp) {
+    const int i = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= dp.npairs || x >= dp.W[i] || y >= dp.H[i]) return;
+    const size_t o = (size_t)y * dp.ld[i] + x;
+    hs_derivs_at(dp.I0[i], dp.I1[i], x, y, dp.H[i], dp.W[i], dp.ld[i], dp.Ix[i][o], dp.Iy[i][o],
+                 dp.It[i][o]);
+    dp.U0[i][o] = 0.0f;
+    dp.V0[i][o] = 0.0f;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Lane 0: wait until tiles (seg+-1, strip+-1) of pair P have completed `need` passes.
+// Returns false if the wait gave up or another warp aborted.
+__device__ bool wait_neighbours(const BatchPair &P, int seg, int strip, unsigned need,
+                                const unsigned *abort_flag) {
+    const int nseg = (P.H + P.seg_rows - 1) / P.seg_rows;
+    unsigned long long polls = 0;
+    unsigned ns = 32;
+    for (int dg = -1; dg <= 1; ++dg) {
+        const int g = seg + dg;
+        if (g < 0 || g >= nseg) continue;
+        for (int ds = -1; ds <= 1; ++ds) {
+            const int s = strip + ds;
+            if (s < 0 || s >= P.nstrips) continue;
+            const unsigned *flag = P.progress + (size_t)g * P.nstrips + s;
+            while (ld_acquire(flag) < need) {
+                if (++polls > kWaitPolls) return false;
+                if ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag) return false;
+                __nanosleep(ns);
+                ns = min(ns * 2, 1024u);
+            }
+        }
+    }
+    return true;
+}
+
+// (pass, pair, local tile) of work item `g`.
+__device__ __forceinline__ void decode(const BatchParams &bp, int g, int &pass, int &pair, int &local) {
+    int j = 0;
+    while (j + 1 < bp.ngroups && g >= bp.g_first[j + 1]) ++j;
+    const int per_pass = bp.item_prefix[bp.g_active[j]];
+    const int r = g - bp.g_first[j];
+    pass = bp.g_p0[j] + r / per_pass;
+    const int t = r % per_pass;
+    int lo = 0, hi = bp.g_active[j] - 1;  // largest i with item_prefix[i] <= t
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (bp.item_prefix[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    pair = lo;
+    local = t - bp.item_prefix[lo];
+}
+
+template <int T, bool FAST>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3 : 2)))
+    hs_batch_kernel(const __grid_constant__ BatchParams bp) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * Geo<T>::warp_floats;
+
+    griddep_launch_dependents();
+    griddep_wait();
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = (int)atomicAdd(bp.queue, 1u);
+        g = __shfl_sync(kFull, g, 0);
+        if (g >= bp.total_items) break;
+        int pass, pi, local;
+        decode(bp, g, pass, pi, local);
+        const BatchPair &P = bp.pair[pi];
+        const int strip = local % P.nstrips;
+        const int seg = local / P.nstrips;
+        int ok = 1;
+        if (lane == 0) {
+            ok = (*(volatile const unsigned *)bp.abort_flag == 0);
+            if (ok && pass > 0) ok = wait_neighbours(P, seg, strip, (unsigned)pass, bp.abort_flag);
+            if (!ok) {
+                atomicCAS(bp.status, 0, (int)HS_ERR_TIMEOUT);
+                atomicExch(bp.abort_flag, 1u);
+            }
+        }
+        ok = __shfl_sync(kFull, ok, 0);
+        if (!ok) break;
+        __syncwarp();
+
+        SweepParams sp;
+        const int src = (P.start + pass) & 1;
+        sp.Ix = P.Ix;
+        sp.Iy = P.Iy;
+        sp.It = P.It;
+        sp.u_in = P.U[src];
+        sp.v_in = P.V[src];
+        sp.u_out = P.U[src ^ 1];
+        sp.v_out = P.V[src ^ 1];
+        sp.H = P.H;
+        sp.W = P.W;
+        sp.ld = P.ld;
+        sp.alpha2 = P.alpha2;
+        sp.we = bp.we;
+        sp.wc = bp.wc;
+        sp.seg_rows = P.seg_rows;
+        sp.nstrips = P.nstrips;
+        sp.nitems = P.items;
+        Item it;
+        init_item<T>(it, sp, strip, seg, lane, wbase);
+        run_item<T, FAST>(sp, it);
+
+        // every lane makes its own stores visible GPU-wide before the warp publishes
+        __threadfence();
+        __syncwarp();
+        if (lane == 0) st_release(P.progress + (size_t)seg * P.nstrips + strip, (unsigned)(pass + 1));
+    }
+}
+
+// ------------------------------------------------------------------ host side
+
+struct PairPlan {
+    int idx;  // position in the caller's array
+    int H, W, ld, iters, passes, rem, start, nstrips, seg_rows, nseg, items;
+    size_t off_planes, off_progress;
+};
+
+static int batch_seg_rows(int H, int T, int cfg_rows) {
+    if (cfg_rows > 0) return std::max(std::min(cfg_rows, H), std::min(H, T));
+    return std::min(H, std::max(64, T));
+}
+
+static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *cfg,
+                            ResolvedConfig &rc, std::vector<PairPlan> &plan, size_t &total) {
+    hs_status st = resolve_config(cfg, &rc);
+    if (st != HS_OK) return st;
+    if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
+    if (n < 1 || n > kMaxBatch) HS_FAIL(HS_ERR_INVALID_ARG, "n=%d outside 1..%d", n, kMaxBatch);
+    const int T = rc.T;
+    plan.clear();
+    size_t off = kHeaderBytes;
+    for (int i = 0; i < n; ++i) {
+        const hs_pair_desc &d = pairs[i];
+        if ((st = check_plane_geometry(d.H, d.W, d.ld)) != HS_OK) return st;
+        if (d.iters < 0) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: iters=%d < 0", i, d.iters);
+        if (d.reserved != 0) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: reserved must be zero", i);
+        PairPlan p;
+        p.idx = i;
+        p.H = d.H;
+        p.W = d.W;
+        p.ld = d.ld;
+        p.iters = d.iters;
+        p.passes = d.iters / T;
+        p.rem = d.iters % T;
+        const int total_passes = p.passes + (p.rem ? 1 : 0);
+        p.start = total_passes & 1;  // the last pass writes buffer 0, the caller's u, v
+        p.nstrips = (d.W + strip_cols_for(T) - 1) / strip_cols_for(T);
+        p.seg_rows = batch_seg_rows(d.H, T, rc.seg_rows);
+        p.nseg = (d.H + p.seg_rows - 1) / p.seg_rows;
+        p.items = p.nstrips * p.nseg;
+        p.off_planes = off;
+        off += 5 * round_up(plane_bytes(d.H, d.ld), 256);
+        plan.push_back(p);
+    }
+    for (auto &p : plan) {
+        p.off_progress = off;
+        off += round_up(sizeof(unsigned) * (size_t)p.items, 16);
+    }
+    total = round_up(off, 256);
+    return HS_OK;
+}
+
+template <int T, bool FAST>
+static hs_status launch_batch(const BatchParams &bp, cudaStream_t stream) {
+    auto fn = hs_batch_kernel<T, FAST>;
+    static std::mutex mu;
+    static int blocks_per_sm[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    int bps = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (dev < 64 && blocks_per_sm[dev] == 0) {
+            HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               Geo<T>::smem_bytes));
+            int b = 0;
+            HS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kWarpsPerBlock * 32,
+                                                                        Geo<T>::smem_bytes));
+            blocks_per_sm[dev] = std::max(b, 1);
+        }
+        bps = dev < 64 ? blocks_per_sm[dev] : 1;
+    }
+    const long want = (long)sm_count() * bps;
+    const long need = ((long)bp.total_items + kWarpsPerBlock - 1) / kWarpsPerBlock;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)std::max(1L, std::min(want, need)));
+    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.dynamicSmemBytes = Geo<T>::smem_bytes;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, fn, bp));
+    return HS_OK;
+}
+
+static hs_status launch_batch_any(int T, bool fast, const BatchParams &bp, cudaStream_t s) {
+#define HS_CASE(TT)                                                                 \
+    case TT: return fast ? launch_batch<TT, true>(bp, s) : launch_batch<TT, false>(bp, s);
+    switch (T) {
+        HS_CASE(1) HS_CASE(2) HS_CASE(3) HS_CASE(4) HS_CASE(5) HS_CASE(6) HS_CASE(7) HS_CASE(8)
+    }
+#undef HS_CASE
+    HS_FAIL(HS_ERR_INVALID_ARG, "sweeps_per_pass=%d outside 1..%d", T, HS_MAX_SWEEPS_PER_PASS);
+}
+
+}  // namespace hs
+
+using namespace hs;
+
+extern "C" {
+
+size_t hs_forward_batched_workspace_bytes(const hs_pair_desc *pairs, int n, const hs_config *cfg) {
+    ResolvedConfig rc;
+    std::vector<PairPlan> plan;
+    size_t total = 0;
+    if (plan_batch(pairs, n, cfg, rc, plan, total) != HS_OK) return 0;
+    return total;
+}
+
+hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
+                             size_t workspace_bytes, const hs_config *cfg, int *device_status,
+                             void *stream) {
+    clear_error();
+    ResolvedConfig rc;
+    std::vector<PairPlan> plan;
+    size_t total = 0;
+    hs_status st = plan_batch(pairs, n, cfg, rc, plan, total);
+    if (st != HS_OK) return st;
+    if (!workspace || workspace_bytes < total)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, total);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+        HS_FAIL(HS_ERR_ALIGNMENT, "workspace is not 256-byte aligned");
+    for (int i = 0; i < n; ++i) {
+        const hs_pair_desc &d = pairs[i];
+        const void *pl[4] = {d.I0, d.I1, d.u, d.v};
+        const char *nm[4] = {"I0", "I1", "u", "v"};
+        for (int k = 0; k < 4; ++k)
+            if ((st = check_plane(pl[k], nm[k])) != HS_OK) {
+                set_error("pair %d: %s", i, hs_last_error());
+                return st;
+            }
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    char *ws = reinterpret_cast<char *>(workspace);
+    unsigned *queue = reinterpret_cast<unsigned *>(ws);
+    int *status = device_status ? device_status : reinterpret_cast<int *>(ws + 4);
+    unsigned *abort_flag = reinterpret_cast<unsigned *>(ws + 8);
+
+    // header and every pair's tile-progress counters start at zero
+    HS_CUDA_CHECK(cudaMemsetAsync(ws, 0, kHeaderBytes, s));
+    if (device_status) HS_CUDA_CHECK(cudaMemsetAsync(device_status, 0, sizeof(int), s));
+    const size_t prog_begin = plan.front().off_progress;
+    HS_CUDA_CHECK(cudaMemsetAsync(ws + prog_begin, 0, total - prog_begin, s));
+
+    // pair buffers
+    std::vector<BatchPair> bpairs(n);
+    DerivParams dp;
+    memset(&dp, 0, sizeof(dp));
+    dp.npairs = n;
+    int maxW = 1, maxH = 1;
+    for (int i = 0; i < n; ++i) {
+        const PairPlan &p = plan[i];
+        const hs_pair_desc &d = pairs[i];
+        const size_t pb = round_up(plane_bytes(p.H, p.ld), 256);
+        float *base = reinterpret_cast<float *>(ws + p.off_planes);
+        BatchPair &b = bpairs[i];
+        b.Ix = base;
+        b.Iy = reinterpret_cast<float *>(ws + p.off_planes + pb);
+        b.It = reinterpret_cast<float *>(ws + p.off_planes + 2 * pb);
+        b.U[0] = d.u;
+        b.V[0] = d.v;
+        b.U[1] = reinterpret_cast<float *>(ws + p.off_planes + 3 * pb);
+        b.V[1] = reinterpret_cast<float *>(ws + p.off_planes + 4 * pb);
+        b.progress = reinterpret_cast<unsigned *>(ws + p.off_progress);
+        b.H = p.H;
+        b.W = p.W;
+        b.ld = p.ld;
+        b.alpha2 = d.alpha * d.alpha;
+        b.passes = p.passes;
+        b.start = p.start;
+        b.nstrips = p.nstrips;
+        b.seg_rows = p.seg_rows;
+        b.items = p.items;
+        dp.I0[i] = d.I0;
+        dp.I1[i] = d.I1;
+        dp.Ix[i] = const_cast<float *>(b.Ix);
+        dp.Iy[i] = const_cast<float *>(b.Iy);
+        dp.It[i] = const_cast<float *>(b.It);
+        dp.U0[i] = b.U[p.start];
+        dp.V0[i] = b.V[p.start];
+        dp.H[i] = p.H;
+        dp.W[i] = p.W;
+        dp.ld[i] = p.ld;
+        maxW = std::max(maxW, p.W);
+        maxH = std::max(maxH, p.H);
+    }
+    {
+        dim3 block(64, 4);
+        dim3 grid((unsigned)((maxW + 63) / 64), (unsigned)((maxH + 3) / 4), (unsigned)n);
+        batch_derivs_kernel<<<grid, block, 0, s>>>(dp);
+        HS_LAUNCH_CHECK("batch_derivs_kernel");
+    }
+
+    // persistent kernel over every full pass of every pair
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return bpairs[a].passes > bpairs[b].passes; });
+    BatchParams bp;
+    memset(&bp, 0, sizeof(bp));
+    bp.npairs = n;
+    bp.we = rc.we;
+    bp.wc = rc.wc;
+    bp.queue = queue;
+    bp.status = status;
+    bp.abort_flag = abort_flag;
+    bp.item_prefix[0] = 0;
+    for (int r = 0; r < n; ++r) {
+        bp.pair[r] = bpairs[order[r]];
+        bp.item_prefix[r + 1] = bp.item_prefix[r] + bp.pair[r].items;
+    }
+    // pass groups: runs of passes with the same number of active (sorted) pairs
+    long total_items = 0;
+    int ng = 0, p0 = 0;
+    for (int r = n; r >= 1; --r) {
+        const int p1 = bp.pair[r - 1].passes;  // the first r pairs are active for p < p1
+        if (p1 > p0) {
+            bp.g_p0[ng] = p0;
+            bp.g_p1[ng] = p1;
+            bp.g_active[ng] = r;
+            bp.g_first[ng] = (int)total_items;
+            total_items += (long)(p1 - p0) * bp.item_prefix[r];
+            ++ng;
+            p0 = p1;
+        }
+    }
+    if (total_items > 0x7fffffffL) HS_FAIL(HS_ERR_UNSUPPORTED, "batch has too many work items");
+    bp.ngroups = ng;
+    bp.total_items = (int)total_items;
+    if (total_items > 0)
+        if ((st = launch_batch_any(rc.T, rc.fast, bp, s)) != HS_OK) return st;
+
+    // the short last pass of pairs whose sweep count is not a multiple of T
+    for (int i = 0; i < n; ++i) {
+        const PairPlan &p = plan[i];
+        if (p.rem == 0) continue;
+        const BatchPair &b = bpairs[i];
+        const int src = (p.start + p.passes) & 1;
+        SweepParams pp;
+        pp.Ix = b.Ix;
+        pp.Iy = b.Iy;
+        pp.It = b.It;
+        pp.u_in = b.U[src];
+        pp.v_in = b.V[src];
+        pp.u_out = b.U[src ^ 1];
+        pp.v_out = b.V[src ^ 1];
+        pp.H = p.H;
+        pp.W = p.W;
+        pp.ld = p.ld;
+        pp.alpha2 = b.alpha2;
+        pp.we = rc.we;
+        pp.wc = rc.wc;
+        const int sc = strip_cols_for(p.rem);
+        pp.nstrips = (p.W + sc - 1) / sc;
+        pp.seg_rows = default_seg_rows(p.H, pp.nstrips, p.rem);
+        pp.nitems = pp.nstrips * ((p.H + pp.seg_rows - 1) / pp.seg_rows);
+        if ((st = launch_pass(p.rem, rc.fast, pp, s)) != HS_OK) return st;
+    }
+    return HS_OK;
+}
+
+}  // extern "C"

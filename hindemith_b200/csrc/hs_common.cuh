@@ -64,4 +64,36 @@ int sm_count();
 constexpr float kAvgCorner = (float)(1.0 / 12.0);
 constexpr float kAvgEdge = (float)(1.0 / 6.0);
 
+#ifdef __CUDACC__
+// Horn-Schunck 2x2x2 derivatives at (x, y).  Tap order (0,0) (1,0) (0,1) (1,1), taps
+// clamped to the image; each accumulator sums from 0 in that order, one rounding per
+// operation; then Ix = DxI0 + DxI1, Iy = DyI0 + DyI1, It = DtI1 - DtI0.
+__device__ __forceinline__ void hs_derivs_at(const float *__restrict__ I0,
+                                             const float *__restrict__ I1, int x, int y, int H,
+                                             int W, int ld, float &Ix, float &Iy, float &It) {
+    const int x1 = min(x + 1, W - 1);
+    const int y1 = min(y + 1, H - 1);
+    const size_t r0 = (size_t)y * ld, r1 = (size_t)y1 * ld;
+    const float a[4] = {__ldg(I0 + r0 + x), __ldg(I0 + r0 + x1), __ldg(I0 + r1 + x),
+                        __ldg(I0 + r1 + x1)};
+    const float b[4] = {__ldg(I1 + r0 + x), __ldg(I1 + r0 + x1), __ldg(I1 + r1 + x),
+                        __ldg(I1 + r1 + x1)};
+    const float wx[4] = {-0.25f, 0.25f, -0.25f, 0.25f};
+    const float wy[4] = {-0.25f, -0.25f, 0.25f, 0.25f};
+    float ax0 = 0.f, ax1 = 0.f, ay0 = 0.f, ay1 = 0.f, at0 = 0.f, at1 = 0.f;
+#pragma unroll
+    for (int d = 0; d < 4; ++d) {
+        ax0 = __fadd_rn(ax0, __fmul_rn(wx[d], a[d]));
+        ax1 = __fadd_rn(ax1, __fmul_rn(wx[d], b[d]));
+        ay0 = __fadd_rn(ay0, __fmul_rn(wy[d], a[d]));
+        ay1 = __fadd_rn(ay1, __fmul_rn(wy[d], b[d]));
+        at0 = __fadd_rn(at0, __fmul_rn(0.25f, a[d]));
+        at1 = __fadd_rn(at1, __fmul_rn(0.25f, b[d]));
+    }
+    Ix = __fadd_rn(ax0, ax1);
+    Iy = __fadd_rn(ay0, ay1);
+    It = __fsub_rn(at1, at0);
+}
+#endif
+
 }  // namespace hs

@@ -94,9 +94,7 @@ __global__ void __launch_bounds__(256) pointwise_kernel(int mode, int op,
     a[i] = r;
 }
 
-// Horn-Schunck 2x2x2 derivatives, one pass.  Tap order (0,0) (1,0) (0,1) (1,1); each
-// accumulator sums from 0 in that order, then Ix = DxI0 + DxI1, Iy = DyI0 + DyI1,
-// It = DtI1 - DtI0.
+// Horn-Schunck 2x2x2 derivatives, one pass (hs_derivs_at in hs_common.cuh).
 __global__ void __launch_bounds__(256) derivs_kernel(const float *__restrict__ I0,
                                                      const float *__restrict__ I1,
                                                      float *__restrict__ Ix,
@@ -106,28 +104,8 @@ __global__ void __launch_bounds__(256) derivs_kernel(const float *__restrict__ I
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
-    const int x1 = min(x + 1, W - 1);
-    const int y1 = min(y + 1, H - 1);
-    const size_t r0 = (size_t)y * ld, r1 = (size_t)y1 * ld;
-    const float a[4] = {__ldg(I0 + r0 + x), __ldg(I0 + r0 + x1), __ldg(I0 + r1 + x),
-                        __ldg(I0 + r1 + x1)};
-    const float b[4] = {__ldg(I1 + r0 + x), __ldg(I1 + r0 + x1), __ldg(I1 + r1 + x),
-                        __ldg(I1 + r1 + x1)};
-    const float wx[4] = {-0.25f, 0.25f, -0.25f, 0.25f};
-    const float wy[4] = {-0.25f, -0.25f, 0.25f, 0.25f};
-    float ax0 = 0.f, ax1 = 0.f, ay0 = 0.f, ay1 = 0.f, at0 = 0.f, at1 = 0.f;
-#pragma unroll
-    for (int d = 0; d < 4; ++d) {
-        ax0 = __fadd_rn(ax0, __fmul_rn(wx[d], a[d]));
-        ax1 = __fadd_rn(ax1, __fmul_rn(wx[d], b[d]));
-        ay0 = __fadd_rn(ay0, __fmul_rn(wy[d], a[d]));
-        ay1 = __fadd_rn(ay1, __fmul_rn(wy[d], b[d]));
-        at0 = __fadd_rn(at0, __fmul_rn(0.25f, a[d]));
-        at1 = __fadd_rn(at1, __fmul_rn(0.25f, b[d]));
-    }
-    Ix[r0 + x] = __fadd_rn(ax0, ax1);
-    Iy[r0 + x] = __fadd_rn(ay0, ay1);
-    It[r0 + x] = __fsub_rn(at1, at0);
+    const size_t i = (size_t)y * ld + x;
+    hs_derivs_at(I0, I1, x, y, H, W, ld, Ix[i], Iy[i], It[i]);
 }
 
 static inline dim3 grid2d(int H, int W, dim3 block) {

@@ -126,6 +126,38 @@ HS_API hs_status hs_forward(const float *I0, const float *I1, int H, int W, int 
                      int iters, float *u, float *v, void *workspace, size_t workspace_bytes,
                      const hs_config *cfg, void *stream);
 
+/* ---- batched Horn-Schunck ---------------------------------------------------- */
+
+#define HS_MAX_BATCH 128
+
+/* One image pair of a batch.  Device pointers; each pair has its own size, alpha and
+ * sweep count. */
+typedef struct hs_pair_desc {
+    const float *I0, *I1;  /* inputs, H x ld planes */
+    float *u, *v;          /* outputs, H x ld planes */
+    int H, W, ld;
+    float alpha;           /* alpha2 = alpha * alpha */
+    int iters;             /* Jacobi sweeps, >= 0 */
+    int reserved;          /* must be zero */
+} hs_pair_desc;
+
+/* Workspace hs_forward_batched needs for these pairs and config (0 if they are invalid):
+ * five planes per pair plus one counter per work tile and a 256-byte header. */
+HS_API size_t hs_forward_batched_workspace_bytes(const hs_pair_desc *pairs, int n,
+                                                 const hs_config *cfg);
+
+/* hs_forward for n (1..HS_MAX_BATCH) pairs of uneven size in one persistent launch:
+ * every (pass, pair, tile) is a work item taken from a device queue; a tile waits only
+ * for its neighbours' previous pass (bounded waits).  Results equal hs_forward per pair.
+ * Stream-ordered and free of host synchronisation, allocation and pageable copies, so it
+ * can be captured in a CUDA graph (make one call before capturing: the first call sets
+ * kernel attributes).  `device_status` (device int, may be NULL) receives HS_OK or
+ * HS_ERR_TIMEOUT when the stream reaches the end of the call.  The workspace must be
+ * 256-byte aligned.  Replaces looping backend.run over the pairs (backend.cpp:320). */
+HS_API hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
+                                    size_t workspace_bytes, const hs_config *cfg,
+                                    int *device_status, void *stream);
+
 /* ---- allocation-free forward ------------------------------------------------- */
 
 /* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for

@@ -103,3 +103,29 @@ def test_hs_error_raises_with_detail():
         L.check(L.lib().hs_array2d_op(9, fake_ptr(), fake_ptr(), fake_ptr(), 4, 4, 4, None), "hs_array2d_op")
     assert ei.value.status == L.HS_ERR_INVALID_ARG
     assert "op=9" in str(ei.value)
+
+
+def test_batched_workspace_and_argument_checks():
+    from hindemith_b200 import batched
+
+    lib = L.lib()
+    cfg = L.make_config(sweeps_per_pass=4)
+    specs = [(240, 320, 1.0, 100), (7, 130, 0.5, 9)]
+    nb = batched.workspace_bytes(specs, cfg)
+    # header + 5 planes per pair + one counter per (segment, strip) tile
+    planes = 5 * (240 * 320 * 4) + 5 * ((7 * 132 * 4 + 255) // 256 * 256)
+    assert nb >= 256 + planes and nb % 256 == 0
+    arr = (L.hs_pair_desc * 2)()
+    for d, (H, W, a, n) in zip(arr, specs):
+        d.H, d.W, d.ld, d.alpha, d.iters = H, W, (W + 3) // 4 * 4, a, n
+    p = ctypes.c_void_p(0x100000)
+    # n out of range, workspace too small, reserved != 0: rejected before device work
+    assert lib.hs_forward_batched(arr, 0, p, nb, ctypes.byref(cfg), None, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_forward_batched(arr, 129, p, nb, ctypes.byref(cfg), None, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_forward_batched(arr, 2, p, nb - 1, ctypes.byref(cfg), None, None) == L.HS_ERR_WORKSPACE
+    arr[1].reserved = 1
+    assert lib.hs_forward_batched_workspace_bytes(arr, 2, ctypes.byref(cfg)) == 0
+    assert lib.hs_forward_batched(arr, 2, p, nb, ctypes.byref(cfg), None, None) == L.HS_ERR_INVALID_ARG
+    arr[1].reserved = 0
+    arr[0].iters = -1
+    assert lib.hs_forward_batched(arr, 2, p, nb, ctypes.byref(cfg), None, None) == L.HS_ERR_INVALID_ARG
