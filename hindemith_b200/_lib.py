@@ -90,6 +90,14 @@ SIGNATURES = {
     "hs_forward_noalloc": (_i, [_vp, _vp, _i, _i, _i, _f, _i, _vp, _vp, _cfgp, _vp]),
     "hs_forward_batched_workspace_bytes": (_sz, [_pdp, _i, _cfgp]),
     "hs_forward_batched": (_i, [_pdp, _i, _vp, _sz, _cfgp, _vp, _vp]),
+    "hs_derivs_bytes": (_sz, [_i, _i, _i]),
+    "hs_checkpoint_bytes": (_sz, [_i, _i, _i, _i, _i]),
+    "hs_forward_train_workspace_bytes": (_sz, [_i, _i, _i]),
+    "hs_forward_train": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz,
+                              _cfgp, _vp]),
+    "hs_backward_workspace_bytes": (_sz, [_i, _i, _i, _i]),
+    "hs_backward": (_i, [_vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
+                         _cfgp, _vp]),
 }
 
 HS_NOALLOC_SCRATCH_BYTES = 48 << 20

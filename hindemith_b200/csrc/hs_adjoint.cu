@@ -1,0 +1,388 @@
+// hs_adjoint.cu -- reverse mode of the Horn-Schunck forward: gradients of a loss on
+// (u, v) with respect to both images and alpha, with (u, v) checkpointed every
+// `ckpt_every` sweeps and recomputed in between.
+//
+// Forward sweep k (state x_k = (u_k, v_k)):
+//   ubar = A u_k, vbar = A v_k, r = Ix ubar + Iy vbar + It, d = alpha^2 + Ix^2 + Iy^2,
+//   t = r / d, u_{k+1} = ubar - Ix t, v_{k+1} = vbar - Iy t.
+// Its adjoint, given lambda = dL/d(u_{k+1}, v_{k+1}):
+//   g = Ix lu + Iy lv, lr = -g / d, ld = g t / d
+//   dIx += -lu t + lr ubar + 2 Ix ld,  dIy += -lv t + lr vbar + 2 Iy ld,  dIt += lr,
+//   dalpha2 += ld,  lambda <- A^T (lu + lr Ix, lv + lr Iy).
+// The lambda recursion does not involve the state; only the accumulations do, through
+// ubar, vbar and t of sweep k, which is why the states of a checkpoint interval are
+// recomputed (forward kernel, one sweep per pass) before that interval's adjoint sweeps.
+// Finally the derivative stencils' transposes give dI0 = Dx^T dIx + Dy^T dIy - Dt^T dIt,
+// dI1 = Dx^T dIx + Dy^T dIy + Dt^T dIt, and dalpha = 2 alpha sum(dalpha2).
+//
+// A^T of a clamp-to-edge stencil is computed as a gather: output p collects, for every
+// tap (o_x, o_y, w), w times the inputs q with clamp(q + o) == p -- one q in the
+// interior, two or none on an image side ("edge folding").
+#include <algorithm>
+#include <vector>
+
+#include "hs_stream.cuh"
+
+namespace hs {
+
+constexpr int kAdjBX = 32, kAdjBY = 8;
+
+// Positions x (at most 2) with clamp(x + o, 0, n-1) == p, for o in {-1, 0, 1}.
+__device__ __forceinline__ int tap_sources(int p, int o, int n, int xs[2]) {
+    int c = 0;
+    const int x = p - o;
+    if (x >= 0 && x <= n - 1) xs[c++] = x;
+    if (o == -1 && p == 0 && x != 0) xs[c++] = 0;           // 0 + (-1) clamps to 0
+    if (o == 1 && p == n - 1 && x != n - 1) xs[c++] = n - 1;  // (n-1) + 1 clamps to n-1
+    return c;
+}
+
+struct AdjParams {
+    const float *Ix, *Iy, *It;
+    const float *u, *v;          // forward state x_k (input of sweep k)
+    const float *lu_in, *lv_in;  // dL/dx_{k+1}
+    float *lu_out, *lv_out;      // dL/dx_k
+    float *dIx, *dIy, *dIt, *dA2;  // per-pixel accumulators (+=)
+    const float *alpha_dev;
+    int H, W, ld;
+    float we, wc;
+};
+
+__device__ __forceinline__ float avg_at(const float *__restrict__ a, int x, int y, int H, int W,
+                                        int ld, float we, float wc) {
+    const int xm = max(x - 1, 0), xp = min(x + 1, W - 1);
+    const int ym = max(y - 1, 0), yp = min(y + 1, H - 1);
+    const float *r0 = a + (size_t)ym * ld, *r1 = a + (size_t)y * ld, *r2 = a + (size_t)yp * ld;
+    const float edges = (__ldg(r0 + x) + __ldg(r2 + x)) + (__ldg(r1 + xm) + __ldg(r1 + xp));
+    const float corners = (__ldg(r0 + xm) + __ldg(r0 + xp)) + (__ldg(r2 + xm) + __ldg(r2 + xp));
+    return fmaf(we, edges, wc * corners);
+}
+
+// One adjoint sweep.  Block = 32 x 8 pixels; the pointwise part (lu + lr Ix, lv + lr Iy)
+// is formed on the tile plus a 1-pixel halo in shared memory, then A^T gathers from it.
+__global__ void __launch_bounds__(kAdjBX *kAdjBY) hs_adjoint_sweep_kernel(const AdjParams p) {
+    __shared__ float zu[kAdjBY + 2][kAdjBX + 3];
+    __shared__ float zv[kAdjBY + 2][kAdjBX + 3];
+    const int tx = threadIdx.x, ty = threadIdx.y;
+    const int x0 = blockIdx.x * kAdjBX, y0 = blockIdx.y * kAdjBY;
+    const float a = __ldg(p.alpha_dev);
+    const float alpha2 = a * a;
+    for (int i = ty * kAdjBX + tx; i < (kAdjBX + 2) * (kAdjBY + 2); i += kAdjBX * kAdjBY) {
+        const int cy = i / (kAdjBX + 2), cx = i % (kAdjBX + 2);
+        const int gx = x0 + cx - 1, gy = y0 + cy - 1;
+        float za = 0.f, zb = 0.f;
+        if (gx >= 0 && gx < p.W && gy >= 0 && gy < p.H) {
+            const size_t o = (size_t)gy * p.ld + gx;
+            const float ix = __ldg(p.Ix + o), iy = __ldg(p.Iy + o);
+            const float lu = __ldg(p.lu_in + o), lv = __ldg(p.lv_in + o);
+            const float d = fmaf(iy, iy, fmaf(ix, ix, alpha2));
+            const float lr = -fmaf(ix, lu, iy * lv) / d;
+            za = fmaf(lr, ix, lu);
+            zb = fmaf(lr, iy, lv);
+        }
+        zu[cy][cx] = za;
+        zv[cy][cx] = zb;
+    }
+    __syncthreads();
+    const int gx = x0 + tx, gy = y0 + ty;
+    if (gx >= p.W || gy >= p.H) return;
+    const int cx = tx + 1, cy = ty + 1;
+    float su, sv;
+    if (gx >= 1 && gx <= p.W - 2 && gy >= 1 && gy <= p.H - 2) {
+        su = fmaf(p.we, (zu[cy - 1][cx] + zu[cy + 1][cx]) + (zu[cy][cx - 1] + zu[cy][cx + 1]),
+                  p.wc * ((zu[cy - 1][cx - 1] + zu[cy - 1][cx + 1]) + (zu[cy + 1][cx - 1] + zu[cy + 1][cx + 1])));
+        sv = fmaf(p.we, (zv[cy - 1][cx] + zv[cy + 1][cx]) + (zv[cy][cx - 1] + zv[cy][cx + 1]),
+                  p.wc * ((zv[cy - 1][cx - 1] + zv[cy - 1][cx + 1]) + (zv[cy + 1][cx - 1] + zv[cy + 1][cx + 1])));
+    } else {
+        su = 0.f;
+        sv = 0.f;
+        for (int oy = -1; oy <= 1; ++oy) {
+            int ys[2];
+            const int ny = tap_sources(gy, oy, p.H, ys);
+            for (int ox = -1; ox <= 1; ++ox) {
+                if (ox == 0 && oy == 0) continue;
+                const float w = (ox != 0 && oy != 0) ? p.wc : p.we;
+                int xs[2];
+                const int nx = tap_sources(gx, ox, p.W, xs);
+                for (int jy = 0; jy < ny; ++jy)
+                    for (int jx = 0; jx < nx; ++jx) {
+                        su = fmaf(w, zu[ys[jy] - y0 + 1][xs[jx] - x0 + 1], su);
+                        sv = fmaf(w, zv[ys[jy] - y0 + 1][xs[jx] - x0 + 1], sv);
+                    }
+            }
+        }
+    }
+    const size_t o = (size_t)gy * p.ld + gx;
+    p.lu_out[o] = su;
+    p.lv_out[o] = sv;
+
+    // gradient accumulations at this pixel for sweep k
+    const float ix = __ldg(p.Ix + o), iy = __ldg(p.Iy + o), it = __ldg(p.It + o);
+    const float lu = __ldg(p.lu_in + o), lv = __ldg(p.lv_in + o);
+    const float ub = avg_at(p.u, gx, gy, p.H, p.W, p.ld, p.we, p.wc);
+    const float vb = avg_at(p.v, gx, gy, p.H, p.W, p.ld, p.we, p.wc);
+    const float d = fmaf(iy, iy, fmaf(ix, ix, alpha2));
+    const float t = fmaf(ix, ub, fmaf(iy, vb, it)) / d;
+    const float g = fmaf(ix, lu, iy * lv);
+    const float lr = -g / d;
+    const float ld = g * t / d;
+    p.dIx[o] += fmaf(-lu, t, fmaf(lr, ub, 2.f * ix * ld));
+    p.dIy[o] += fmaf(-lv, t, fmaf(lr, vb, 2.f * iy * ld));
+    p.dIt[o] += lr;
+    p.dA2[o] += ld;
+}
+
+// dI0 = Dx^T dIx + Dy^T dIy - Dt^T dIt; dI1 = Dx^T dIx + Dy^T dIy + Dt^T dIt, with the
+// 2x2 derivative taps at offsets (0,0) (1,0) (0,1) (1,1) transposed through their clamps.
+__global__ void __launch_bounds__(256) hs_derivs_adjoint_kernel(const float *__restrict__ dIx,
+                                                                const float *__restrict__ dIy,
+                                                                const float *__restrict__ dIt,
+                                                                float *__restrict__ dI0,
+                                                                float *__restrict__ dI1, int H,
+                                                                int W, int ld) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    const float wx[4] = {-0.25f, 0.25f, -0.25f, 0.25f};
+    const float wy[4] = {-0.25f, -0.25f, 0.25f, 0.25f};
+    const int ox[4] = {0, 1, 0, 1}, oy[4] = {0, 0, 1, 1};
+    float s_common = 0.f, s_t = 0.f;
+    for (int d = 0; d < 4; ++d) {
+        int xs[2], ys[2];
+        const int nx = tap_sources(x, ox[d], W, xs);
+        const int ny = tap_sources(y, oy[d], H, ys);
+        for (int jy = 0; jy < ny; ++jy)
+            for (int jx = 0; jx < nx; ++jx) {
+                const size_t q = (size_t)ys[jy] * ld + xs[jx];
+                s_common = fmaf(wx[d], __ldg(dIx + q), fmaf(wy[d], __ldg(dIy + q), s_common));
+                s_t = fmaf(0.25f, __ldg(dIt + q), s_t);
+            }
+    }
+    const size_t o = (size_t)y * ld + x;
+    dI0[o] = s_common - s_t;
+    dI1[o] = s_common + s_t;
+}
+
+// Deterministic sum of a plane into partials[blockIdx.x] (double), then one block folds
+// the partials: out = 2 * alpha * sum.
+constexpr int kRedBlocks = 256;
+__global__ void __launch_bounds__(256) plane_sum_kernel(const float *__restrict__ a, int H, int W,
+                                                        int ld, double *__restrict__ partials) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    const long n = (long)H * W;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        s += (double)a[(i / W) * ld + (i % W)];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[blockIdx.x] = sh[0];
+}
+
+__global__ void __launch_bounds__(256) fold_dalpha_kernel(const double *__restrict__ partials, int n,
+                                                          const float *__restrict__ alpha_dev,
+                                                          float *__restrict__ dalpha) {
+    __shared__ double sh[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partials[i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *dalpha = (float)(2.0 * (double)__ldg(alpha_dev) * sh[0]);
+}
+
+static inline dim3 grid2(int H, int W, dim3 b) {
+    return dim3((unsigned)((W + b.x - 1) / b.x), (unsigned)((H + b.y - 1) / b.y));
+}
+
+static int n_ckpt(int iters, int every) { return iters <= 0 ? 0 : (iters + every - 1) / every; }
+
+}  // namespace hs
+
+using namespace hs;
+
+extern "C" {
+
+size_t hs_checkpoint_bytes(int H, int W, int ld, int iters, int ckpt_every) {
+    (void)W;
+    if (H < 1 || ld < 1 || iters < 0 || ckpt_every < 1) return 0;
+    return (size_t)n_ckpt(iters, ckpt_every) * 2 * round_up(plane_bytes(H, ld), 256);
+}
+
+size_t hs_derivs_bytes(int H, int W, int ld) {
+    (void)W;
+    if (H < 1 || ld < 1) return 0;
+    return 3 * round_up(plane_bytes(H, ld), 256);
+}
+
+size_t hs_forward_train_workspace_bytes(int H, int W, int ld) { return hs_sweeps_workspace_bytes(H, W, ld); }
+
+hs_status hs_forward_train(const float *I0, const float *I1, int H, int W, int ld,
+                           const float *alpha, int iters, int ckpt_every, float *u, float *v,
+                           float *derivs, float *ckpt, void *workspace, size_t workspace_bytes,
+                           const hs_config *cfg, void *stream) {
+    clear_error();
+    hs_status st = check_plane_geometry(H, W, ld);
+    if (st != HS_OK) return st;
+    const void *planes[6] = {I0, I1, u, v, derivs, ckpt};
+    const char *names[6] = {"I0", "I1", "u", "v", "derivs", "ckpt"};
+    for (int i = 0; i < 6; ++i)
+        if ((i < 5 || iters > 0) && (st = check_plane(planes[i], names[i])) != HS_OK) return st;
+    if (!alpha) HS_FAIL(HS_ERR_INVALID_ARG, "alpha (device pointer) is NULL");
+    if (iters < 0 || ckpt_every < 1) HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d", iters, ckpt_every);
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
+    const size_t need = hs_sweeps_workspace_bytes(H, W, ld);
+    if (iters > 0 && (!workspace || workspace_bytes < need))
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, need);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t pb = round_up(plane_bytes(H, ld), 256);
+    char *dv = reinterpret_cast<char *>(derivs);
+    float *Ix = reinterpret_cast<float *>(dv), *Iy = reinterpret_cast<float *>(dv + pb),
+          *It = reinterpret_cast<float *>(dv + 2 * pb);
+    if ((st = hs_derivs(I0, I1, H, W, ld, Ix, Iy, It, stream)) != HS_OK) return st;
+    HS_CUDA_CHECK(cudaMemsetAsync(u, 0, plane_bytes(H, ld), s));
+    HS_CUDA_CHECK(cudaMemsetAsync(v, 0, plane_bytes(H, ld), s));
+    char *ck = reinterpret_cast<char *>(ckpt);
+    float *u1 = reinterpret_cast<float *>(workspace);
+    float *v1 = reinterpret_cast<float *>(reinterpret_cast<char *>(workspace) + pb);
+    for (int b = 0, done = 0; done < iters; ++b) {
+        HS_CUDA_CHECK(cudaMemcpyAsync(ck + (2 * b) * pb, u, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemcpyAsync(ck + (2 * b + 1) * pb, v, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
+        const int n = std::min(ckpt_every, iters - done);
+        const int passes = (n + rc.T - 1) / rc.T;
+        if (passes % 2 == 1) {
+            HS_CUDA_CHECK(cudaMemcpyAsync(u1, u, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
+            HS_CUDA_CHECK(cudaMemcpyAsync(v1, v, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
+        }
+        if ((st = run_passes_dev(Ix, Iy, It, H, W, ld, 0.f, alpha, n, u, v, u1, v1, rc, s)) != HS_OK)
+            return st;
+        done += n;
+    }
+    return HS_OK;
+}
+
+size_t hs_backward_workspace_bytes(int H, int W, int ld, int ckpt_every) {
+    (void)W;
+    if (H < 1 || ld < 1 || ckpt_every < 1) return 0;
+    const size_t pb = round_up(plane_bytes(H, ld), 256);
+    // recomputed states (2 planes each), lambda ping-pong (4), accumulators (4), partials
+    return (2 * (size_t)ckpt_every + 8) * pb + kRedBlocks * sizeof(double);
+}
+
+hs_status hs_backward(const float *derivs, int H, int W, int ld, const float *alpha, int iters,
+                      int ckpt_every, const float *ckpt, const float *dLdu, const float *dLdv,
+                      float *dI0, float *dI1, float *dalpha, void *workspace,
+                      size_t workspace_bytes, const hs_config *cfg, void *stream) {
+    clear_error();
+    hs_status st = check_plane_geometry(H, W, ld);
+    if (st != HS_OK) return st;
+    const void *planes[6] = {derivs, dLdu, dLdv, dI0, dI1, workspace};
+    const char *names[6] = {"derivs", "dLdu", "dLdv", "dI0", "dI1", "workspace"};
+    for (int i = 0; i < 6; ++i)
+        if ((st = check_plane(planes[i], names[i])) != HS_OK) return st;
+    if (iters > 0 && (st = check_plane(ckpt, "ckpt")) != HS_OK) return st;
+    if (!alpha || !dalpha) HS_FAIL(HS_ERR_INVALID_ARG, "alpha / dalpha (device pointers) NULL");
+    if (iters < 0 || ckpt_every < 1) HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d", iters, ckpt_every);
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
+    const size_t need = hs_backward_workspace_bytes(H, W, ld, ckpt_every);
+    if (workspace_bytes < need)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, need);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t pb = round_up(plane_bytes(H, ld), 256);
+    const size_t pl = plane_bytes(H, ld);
+    char *ws = reinterpret_cast<char *>(workspace);
+    auto P = [&](size_t i) { return reinterpret_cast<float *>(ws + i * pb); };
+    float *states = P(0);  // ckpt_every x (u, v)
+    const size_t base = 2 * (size_t)ckpt_every;
+    float *lam[2][2] = {{P(base), P(base + 1)}, {P(base + 2), P(base + 3)}};
+    float *dIx = P(base + 4), *dIy = P(base + 5), *dIt = P(base + 6), *dA2 = P(base + 7);
+    double *partials = reinterpret_cast<double *>(ws + (base + 8) * pb);
+    const char *dv = reinterpret_cast<const char *>(derivs);
+    const float *Ix = reinterpret_cast<const float *>(dv), *Iy = reinterpret_cast<const float *>(dv + pb),
+                *It = reinterpret_cast<const float *>(dv + 2 * pb);
+
+    HS_CUDA_CHECK(cudaMemcpyAsync(lam[0][0], dLdu, pl, cudaMemcpyDeviceToDevice, s));
+    HS_CUDA_CHECK(cudaMemcpyAsync(lam[0][1], dLdv, pl, cudaMemcpyDeviceToDevice, s));
+    HS_CUDA_CHECK(cudaMemsetAsync(dIx, 0, 4 * pb, s));  // dIx, dIy, dIt, dA2 are adjacent
+    int cur = 0;
+    const int nb = n_ckpt(iters, ckpt_every);
+    for (int b = nb - 1; b >= 0; --b) {
+        const int k_lo = b * ckpt_every;
+        const int n = std::min(ckpt_every, iters - k_lo);
+        const char *ck = reinterpret_cast<const char *>(ckpt);
+        // recompute states x_{k_lo+j}, j = 1..n-1, one sweep per pass
+        std::vector<const float *> su_v(n), sv_v(n);
+        su_v[0] = reinterpret_cast<const float *>(ck + (2 * b) * pb);
+        sv_v[0] = reinterpret_cast<const float *>(ck + (2 * b + 1) * pb);
+        for (int j = 1; j < n; ++j) {
+            SweepParams pp;
+            pp.Ix = Ix;
+            pp.Iy = Iy;
+            pp.It = It;
+            pp.u_in = su_v[j - 1];
+            pp.v_in = sv_v[j - 1];
+            pp.u_out = states + (size_t)(2 * j) * (pb / sizeof(float));
+            pp.v_out = states + (size_t)(2 * j + 1) * (pb / sizeof(float));
+            pp.H = H;
+            pp.W = W;
+            pp.ld = ld;
+            pp.alpha2 = 0.f;
+            pp.alpha_dev = alpha;
+            pp.we = rc.we;
+            pp.wc = rc.wc;
+            const int sc = strip_cols_for(1);
+            pp.nstrips = (W + sc - 1) / sc;
+            pp.seg_rows = default_seg_rows(H, pp.nstrips, 1);
+            pp.nitems = pp.nstrips * ((H + pp.seg_rows - 1) / pp.seg_rows);
+            if ((st = launch_pass(1, rc.fast, pp, s)) != HS_OK) return st;
+            su_v[j] = pp.u_out;
+            sv_v[j] = pp.v_out;
+        }
+        for (int j = n - 1; j >= 0; --j) {
+            AdjParams ap;
+            ap.Ix = Ix;
+            ap.Iy = Iy;
+            ap.It = It;
+            ap.u = su_v[j];
+            ap.v = sv_v[j];
+            ap.lu_in = lam[cur][0];
+            ap.lv_in = lam[cur][1];
+            ap.lu_out = lam[cur ^ 1][0];
+            ap.lv_out = lam[cur ^ 1][1];
+            ap.dIx = dIx;
+            ap.dIy = dIy;
+            ap.dIt = dIt;
+            ap.dA2 = dA2;
+            ap.alpha_dev = alpha;
+            ap.H = H;
+            ap.W = W;
+            ap.ld = ld;
+            ap.we = rc.we;
+            ap.wc = rc.wc;
+            const dim3 blk(kAdjBX, kAdjBY);
+            hs_adjoint_sweep_kernel<<<grid2(H, W, blk), blk, 0, s>>>(ap);
+            HS_LAUNCH_CHECK("hs_adjoint_sweep_kernel");
+            cur ^= 1;
+        }
+    }
+    {
+        const dim3 blk(64, 4);
+        hs_derivs_adjoint_kernel<<<grid2(H, W, blk), blk, 0, s>>>(dIx, dIy, dIt, dI0, dI1, H, W, ld);
+        HS_LAUNCH_CHECK("hs_derivs_adjoint_kernel");
+        plane_sum_kernel<<<kRedBlocks, 256, 0, s>>>(dA2, H, W, ld, partials);
+        HS_LAUNCH_CHECK("plane_sum_kernel");
+        fold_dalpha_kernel<<<1, 256, 0, s>>>(partials, kRedBlocks, alpha, dalpha);
+        HS_LAUNCH_CHECK("fold_dalpha_kernel");
+    }
+    return HS_OK;
+}
+
+}  // extern "C"

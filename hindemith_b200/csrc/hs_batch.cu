@@ -177,6 +177,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
         sp.W = P.W;
         sp.ld = P.ld;
         sp.alpha2 = P.alpha2;
+        sp.alpha_dev = nullptr;
         sp.we = bp.we;
         sp.wc = bp.wc;
         sp.seg_rows = P.seg_rows;
@@ -447,6 +448,7 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
         pp.W = p.W;
         pp.ld = p.ld;
         pp.alpha2 = b.alpha2;
+        pp.alpha_dev = nullptr;
         pp.we = rc.we;
         pp.wc = rc.wc;
         const int sc = strip_cols_for(p.rem);

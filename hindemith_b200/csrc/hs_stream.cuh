@@ -56,6 +56,7 @@ struct SweepParams {
     float *u_out, *v_out;
     int H, W, ld;
     float alpha2;
+    const float *alpha_dev;  // if set, alpha2 = alpha_dev[0] squared (device-resident alpha)
     float we, wc;  // edge and corner weights of the average
     int seg_rows;
     int nstrips;
@@ -153,6 +154,7 @@ struct Item {
     int lcol;      // first column of this lane's 16-byte chunk (clamped into the row)
     bool a_first, a_last, b_last, st_a, st_b;
     int xa, y_start, y_end;
+    float alpha2;  // p.alpha2, or the square of the device-resident alpha
 };
 
 // A row of the strip is 5 planes x 64 floats = 80 chunks of 16 bytes; lane l copies
@@ -192,11 +194,11 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
         const float2 t2 = lds2(raw + 4 * kWarpCols);
         float ax, ay;
         if constexpr (FAST) {
-            ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, p.alpha2)));
-            ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, p.alpha2)));
+            ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
+            ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
         } else {
-            ax = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.x, ix.x)), __fmul_rn(iy.x, iy.x));
-            ay = __fadd_rn(__fadd_rn(p.alpha2, __fmul_rn(ix.y, ix.y)), __fmul_rn(iy.y, iy.y));
+            ax = __fadd_rn(__fadd_rn(it.alpha2, __fmul_rn(ix.x, ix.x)), __fmul_rn(iy.x, iy.x));
+            ay = __fadd_rn(__fadd_rn(it.alpha2, __fmul_rn(ix.y, ix.y)), __fmul_rn(iy.y, iy.y));
         }
         float4 *cs = it.coef + cslot * 64 + it.lane;
         cs[0] = make_float4(ix.x, iy.x, t2.x, ax);
@@ -320,6 +322,11 @@ hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out);
 int strip_cols_for(int T);
 int default_seg_rows(int H, int nstrips, int T);
 hs_status launch_pass(int T, bool fast, const SweepParams &pp, cudaStream_t s);
+// `iters` sweeps; the state starts in (u0, v0) for an even number of passes, in (u1, v1)
+// for an odd one, and always ends in (u0, v0).  alpha_dev, if set, overrides alpha2.
+hs_status run_passes_dev(const float *Ix, const float *Iy, const float *It, int H, int W, int ld,
+                         float alpha2, const float *alpha_dev, int iters, float *u0, float *v0,
+                         float *u1, float *v1, const ResolvedConfig &rc, cudaStream_t stream);
 inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 // Fill the per-warp context for (strip, seg) of the pass described by p.
@@ -346,6 +353,7 @@ __device__ __forceinline__ void init_item(Item &it, const SweepParams &p, int st
     it.st_b = (xb >= vlo && xb < vhi);
     it.y_start = seg * p.seg_rows;
     it.y_end = min(p.H, it.y_start + p.seg_rows);
+    it.alpha2 = p.alpha_dev ? __fmul_rn(__ldg(p.alpha_dev), __ldg(p.alpha_dev)) : p.alpha2;
 }
 
 // Run one work item; only strips reaching an image side need the horizontal clamps.

@@ -119,9 +119,9 @@ hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out) {
 
 // Runs `iters` sweeps.  State starts in (u0, v0) if `start_in_user`, else in (u1, v1);
 // the final state always lands in (u0, v0).
-static hs_status run_passes(const float *Ix, const float *Iy, const float *It, int H, int W,
-                            int ld, float alpha2, int iters, float *u0, float *v0, float *u1,
-                            float *v1, const ResolvedConfig &rc, cudaStream_t stream) {
+hs_status run_passes_dev(const float *Ix, const float *Iy, const float *It, int H, int W, int ld,
+                         float alpha2, const float *alpha_dev, int iters, float *u0, float *v0,
+                         float *u1, float *v1, const ResolvedConfig &rc, cudaStream_t stream) {
     if (iters <= 0) return HS_OK;
     const int T = rc.T;
     const int passes = (iters + T - 1) / T;
@@ -137,6 +137,7 @@ static hs_status run_passes(const float *Ix, const float *Iy, const float *It, i
         pp.u_out = U[1 - cur]; pp.v_out = V[1 - cur];
         pp.H = H; pp.W = W; pp.ld = ld;
         pp.alpha2 = alpha2;
+        pp.alpha_dev = alpha_dev;
         pp.we = rc.we; pp.wc = rc.wc;
         const int sc = strip_cols_for(t);
         pp.nstrips = (W + sc - 1) / sc;
@@ -197,7 +198,7 @@ hs_status hs_sweeps(const float *Ix, const float *Iy, const float *It, int H, in
         HS_CUDA_CHECK(cudaMemcpyAsync(u1, u, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
         HS_CUDA_CHECK(cudaMemcpyAsync(v1, v, plane_bytes(H, ld), cudaMemcpyDeviceToDevice, s));
     }
-    return run_passes(Ix, Iy, It, H, W, ld, alpha2, iters, u, v, u1, v1, rc, s);
+    return run_passes_dev(Ix, Iy, It, H, W, ld, alpha2, nullptr, iters, u, v, u1, v1, rc, s);
 }
 
 hs_status hs_forward(const float *I0, const float *I1, int H, int W, int ld, float alpha,
@@ -233,7 +234,7 @@ hs_status hs_forward(const float *I0, const float *I1, int H, int W, int ld, flo
     HS_CUDA_CHECK(cudaMemsetAsync(zu, 0, plane_bytes(H, ld), s));
     HS_CUDA_CHECK(cudaMemsetAsync(zv, 0, plane_bytes(H, ld), s));
     const float alpha2 = alpha * alpha;  // one FP32 rounding, as the program's ScalarOp
-    return run_passes(Ix, Iy, It, H, W, ld, alpha2, iters, u, v, u1, v1, rc, s);
+    return run_passes_dev(Ix, Iy, It, H, W, ld, alpha2, nullptr, iters, u, v, u1, v1, rc, s);
 }
 
 }  // extern "C"

@@ -158,6 +158,36 @@ HS_API hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *work
                                     size_t workspace_bytes, const hs_config *cfg,
                                     int *device_status, void *stream);
 
+/* ---- differentiable Horn-Schunck --------------------------------------------- */
+
+/* Bytes of the derivative planes (Ix, Iy, It; three planes, each rounded up to 256
+ * bytes) and of the checkpoints ceil(iters/ckpt_every) x (u, v) kept by the forward. */
+HS_API size_t hs_derivs_bytes(int H, int W, int ld);
+HS_API size_t hs_checkpoint_bytes(int H, int W, int ld, int iters, int ckpt_every);
+HS_API size_t hs_forward_train_workspace_bytes(int H, int W, int ld);
+
+/* hs_forward that also keeps what the backward needs: `derivs` receives Ix, Iy, It and
+ * `ckpt` the state (u, v) before sweeps 0, c, 2c, ... (c = ckpt_every).  `alpha` is a
+ * DEVICE pointer to one float (a learnable alpha never needs a host round trip).
+ * Results equal hs_forward's.  No counterpart in the reference, which has no gradients. */
+HS_API hs_status hs_forward_train(const float *I0, const float *I1, int H, int W, int ld,
+                                  const float *alpha, int iters, int ckpt_every, float *u,
+                                  float *v, float *derivs, float *ckpt, void *workspace,
+                                  size_t workspace_bytes, const hs_config *cfg, void *stream);
+
+HS_API size_t hs_backward_workspace_bytes(int H, int W, int ld, int ckpt_every);
+
+/* Gradients of a loss L(u, v) through the whole forward: given dL/du, dL/dv it writes
+ * dL/dI0, dL/dI1 (planes) and dL/dalpha (one device float).  Each checkpoint interval's
+ * states are recomputed from its checkpoint, then its sweeps are reversed with the
+ * adjoint kernel (transposed clamp-to-edge average, adjoint of the pointwise update);
+ * the derivative stencils are transposed last.  Deterministic. */
+HS_API hs_status hs_backward(const float *derivs, int H, int W, int ld, const float *alpha,
+                             int iters, int ckpt_every, const float *ckpt, const float *dLdu,
+                             const float *dLdv, float *dI0, float *dI1, float *dalpha,
+                             void *workspace, size_t workspace_bytes, const hs_config *cfg,
+                             void *stream);
+
 /* ---- allocation-free forward ------------------------------------------------- */
 
 /* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for

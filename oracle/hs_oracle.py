@@ -34,7 +34,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libhsoracle.so")
 
 # Canonical Horn-Schunck stencils, tap order (offx, offy).  Identical tables live in the
-# CUDA sources and in hindemith_b200.stencils; the tests check that they agree.
+# CUDA sources and in hindemith_b200.hlib; the tests check that they agree.
 AVG_OFFX = np.array([-1, 0, 1, -1, 1, -1, 0, 1], dtype=np.int32)
 AVG_OFFY = np.array([-1, -1, -1, 0, 0, 1, 1, 1], dtype=np.int32)
 AVG_W = np.array([1 / 12 if (ox != 0 and oy != 0) else 1 / 6
@@ -259,3 +259,59 @@ def c_warp(src, ox, oy):
     out = np.empty_like(src)
     lib().hso_warp_f32(src, ox, oy, H, W, out)
     return out
+
+
+# ---------------------------------------------------------------- adjoint (FP64)
+
+def hs_adjoint_f64(I0, I1, alpha, iters, lam_u, lam_v):
+    """Reverse-mode gradient of L = <lam_u, u_K> + <lam_v, v_K> with respect to I0, I1
+    and alpha, in FP64, storing every forward state (small sizes only).
+
+    Forward sweep: ubar = A u; vbar = A v; r = Ix ubar + Iy vbar + It; d = a2 + Ix^2 + Iy^2;
+    t = r / d; u' = ubar - Ix t; v' = vbar - Iy t.  Adjoint of one sweep, given the
+    gradient (lu, lv) of its output: g = Ix lu + Iy lv; lr = -g/d; ld = g t / d;
+    dIx += -lu t + lr ubar + 2 Ix ld; dIy += -lv t + lr vbar + 2 Iy ld; dIt += lr;
+    da2 += ld; (lu, lv) <- A^T (lu + lr Ix, lv + lr Iy).  Then the derivative stencils'
+    transposes map (dIx, dIy, dIt) to (dI0, dI1), and dalpha = 2 alpha da2.
+    """
+    f64 = np.float64
+    I0 = np.asarray(I0, f64)
+    I1 = np.asarray(I1, f64)
+    Ix, Iy, It = hs_derivs(I0, I1, f64)
+    a2 = f64(alpha) * f64(alpha)
+    d = a2 + Ix * Ix + Iy * Iy
+    avg = (AVG_W.astype(f64), AVG_OFFX, AVG_OFFY)
+    u = np.zeros_like(I0)
+    v = np.zeros_like(I0)
+    states = []
+    for _ in range(iters):
+        states.append((u, v))
+        ub = stencil2d(*avg, u, f64)
+        vb = stencil2d(*avg, v, f64)
+        t = (Ix * ub + Iy * vb + It) / d
+        u, v = ub - Ix * t, vb - Iy * t
+    lu = np.asarray(lam_u, f64).copy()
+    lv = np.asarray(lam_v, f64).copy()
+    dIx = np.zeros_like(I0)
+    dIy = np.zeros_like(I0)
+    dIt = np.zeros_like(I0)
+    da2 = 0.0
+    for k in range(iters - 1, -1, -1):
+        uk, vk = states[k]
+        ub = stencil2d(*avg, uk, f64)
+        vb = stencil2d(*avg, vk, f64)
+        t = (Ix * ub + Iy * vb + It) / d
+        g = Ix * lu + Iy * lv
+        lr = -g / d
+        ldd = g * t / d
+        dIx += -lu * t + lr * ub + 2 * Ix * ldd
+        dIy += -lv * t + lr * vb + 2 * Iy * ldd
+        dIt += lr
+        da2 += ldd.sum()
+        lu = stencil2d_transpose(*avg, lu + lr * Ix, f64)
+        lv = stencil2d_transpose(*avg, lv + lr * Iy, f64)
+    dxT = lambda w, z: stencil2d_transpose(w.astype(f64), D_OFFX, D_OFFY, z, f64)  # noqa: E731
+    dI0 = dxT(DX_W, dIx) + dxT(DY_W, dIy) - dxT(DT_W, dIt)
+    dI1 = dxT(DX_W, dIx) + dxT(DY_W, dIy) + dxT(DT_W, dIt)
+    return dI0, dI1, 2.0 * f64(alpha) * da2, (u, v)
+

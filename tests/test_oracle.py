@@ -114,3 +114,28 @@ def test_stencil_transpose_adjoint():
             STy = O.c_stencil2d_transpose(w, ox, oy, y)
             assert abs((Sx * y).sum() - (x * STy).sum()) < 1e-12
             np.testing.assert_allclose(STy, O.stencil2d_transpose(w, ox, oy, y), atol=1e-14)
+
+
+def test_torch_reference_matches_fp64_oracle():
+    """The pure-PyTorch HS used as a gradient reference agrees with the FP64 oracle in
+    both the forward and the reverse mode."""
+    import torch
+
+    from hs_torch_ref import hs_torch
+
+    rng = np.random.default_rng(11)
+    H, W, K = 13, 17, 15
+    from hindemith_b200 import synthetic
+
+    I0, I1, _, _ = synthetic.make_pair(H, W, seed=4)
+    lu, lv = rng.standard_normal((H, W)), rng.standard_normal((H, W))
+    t0 = torch.from_numpy(I0.astype(np.float64)).requires_grad_(True)
+    t1 = torch.from_numpy(I1.astype(np.float64)).requires_grad_(True)
+    ta = torch.tensor(0.6, dtype=torch.float64, requires_grad=True)
+    u, v = hs_torch(t0, t1, ta, K)
+    ((u * torch.from_numpy(lu)).sum() + (v * torch.from_numpy(lv)).sum()).backward()
+    r0, r1, ra, (ru, rv) = O.hs_adjoint_f64(I0, I1, 0.6, K, lu, lv)
+    np.testing.assert_allclose(u.detach().numpy(), ru, atol=1e-12)
+    np.testing.assert_allclose(t0.grad.numpy(), r0, atol=1e-10)
+    np.testing.assert_allclose(t1.grad.numpy(), r1, atol=1e-10)
+    assert abs(float(ta.grad) - ra) < 1e-9
