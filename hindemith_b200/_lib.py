@@ -60,6 +60,17 @@ class hs_pair_desc(ctypes.Structure):
 
 HS_MAX_BATCH = 128
 
+
+class hs_train_pair(ctypes.Structure):
+    _fields_ = [("I0", ctypes.c_void_p), ("I1", ctypes.c_void_p), ("u", ctypes.c_void_p),
+                ("v", ctypes.c_void_p), ("alpha", ctypes.c_void_p), ("dLdu", ctypes.c_void_p),
+                ("dLdv", ctypes.c_void_p), ("dI0", ctypes.c_void_p), ("dI1", ctypes.c_void_p),
+                ("dalpha", ctypes.c_void_p), ("H", ctypes.c_int), ("W", ctypes.c_int),
+                ("ld", ctypes.c_int), ("reserved", ctypes.c_int)]
+
+
+HS_MAX_TRAIN_PAIRS = 32
+
 _lib = None
 _lock = threading.Lock()
 
@@ -71,6 +82,7 @@ _ip = ctypes.POINTER(ctypes.c_int)
 _fp = ctypes.POINTER(ctypes.c_float)
 _cfgp = ctypes.POINTER(hs_config)
 _pdp = ctypes.POINTER(hs_pair_desc)
+_tpp = ctypes.POINTER(hs_train_pair)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -96,6 +108,9 @@ SIGNATURES = {
     "hs_forward_train": (_i, [_vp, _vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _sz,
                               _cfgp, _vp]),
     "hs_backward_workspace_bytes": (_sz, [_i, _i, _i, _i]),
+    "hs_train_workspace_bytes": (_sz, [_tpp, _i, _i, _i]),
+    "hs_forward_train_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
+    "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_backward": (_i, [_vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
                          _cfgp, _vp]),
 }

@@ -336,6 +336,7 @@ hs_status hs_backward(const float *derivs, int H, int W, int ld, const float *al
             pp.ld = ld;
             pp.alpha2 = 0.f;
             pp.alpha_dev = alpha;
+            pp.dump = 0;
             pp.we = rc.we;
             pp.wc = rc.wc;
             const int sc = strip_cols_for(1);

@@ -105,7 +105,7 @@ __device__ bool wait_neighbours(const BatchPair &P, int seg, int strip, unsigned
                 if (++polls > kWaitPolls) return false;
                 if ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag) return false;
                 __nanosleep(ns);
-                ns = min(ns * 2, 1024u);
+                ns = min(ns * 2, 256u);
             }
         }
     }
@@ -178,6 +178,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
         sp.ld = P.ld;
         sp.alpha2 = P.alpha2;
         sp.alpha_dev = nullptr;
+        sp.dump = 0;
         sp.we = bp.we;
         sp.wc = bp.wc;
         sp.seg_rows = P.seg_rows;
@@ -449,6 +450,7 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
         pp.ld = p.ld;
         pp.alpha2 = b.alpha2;
         pp.alpha_dev = nullptr;
+        pp.dump = 0;
         pp.we = rc.we;
         pp.wc = rc.wc;
         const int sc = strip_cols_for(p.rem);

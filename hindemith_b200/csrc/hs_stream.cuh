@@ -57,6 +57,8 @@ struct SweepParams {
     int H, W, ld;
     float alpha2;
     const float *alpha_dev;  // if set, alpha2 = alpha_dev[0] squared (device-resident alpha)
+    int dump;                // if set, stage s also writes its sweep into dump_u/v[s]
+    float *dump_u[HS_MAX_SWEEPS_PER_PASS], *dump_v[HS_MAX_SWEEPS_PER_PASS];
     float we, wc;  // edge and corner weights of the average
     int seg_rows;
     int nstrips;
@@ -152,6 +154,7 @@ struct Item {
     float4 *coef;  // [T+1][2][32]
     int lane;
     int lcol;      // first column of this lane's 16-byte chunk (clamped into the row)
+    int lc2;       // the lane's own column pair (xa, xa+1), or any in-bounds pair
     bool a_first, a_last, b_last, st_a, st_b;
     int xa, y_start, y_end;
     float alpha2;  // p.alpha2, or the square of the device-resident alpha
@@ -243,6 +246,19 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
                 const float t = __fdiv_rn(r, C[j].w);
                 cu[0][j] = __fsub_rn(ubar, __fmul_rn(C[j].x, t));
                 cu[1][j] = __fsub_rn(vbar, __fmul_rn(C[j].y, t));
+            }
+        }
+        if (p.dump) {  // warp-uniform: write sweep s+1 of row k-s-1 (state dumps)
+            const int rr = k - s - 1;
+            if (rr >= it.y_start && rr < it.y_end) {
+                const size_t off = (size_t)rr * p.ld + it.xa;
+                if (it.st_a && it.st_b) {
+                    *reinterpret_cast<float2 *>(p.dump_u[s] + off) = make_float2(cu[0][0], cu[0][1]);
+                    *reinterpret_cast<float2 *>(p.dump_v[s] + off) = make_float2(cu[1][0], cu[1][1]);
+                } else if (it.st_a) {
+                    p.dump_u[s][off] = cu[0][0];
+                    p.dump_v[s][off] = cu[1][0];
+                }
             }
         }
     }
@@ -345,6 +361,7 @@ __device__ __forceinline__ void init_item(Item &it, const SweepParams &p, int st
     // feed a stored pixel)
     const int xc = x0 + 4 * (lane & 15);
     it.lcol = (xc >= 0 && xc + 4 <= p.ld) ? xc : 0;
+    it.lc2 = (it.xa >= 0 && it.xa < p.W) ? it.xa : 0;  // xa is even and ld % 4 == 0
     it.a_first = (it.xa == 0);
     it.a_last = (it.xa == p.W - 1);
     it.b_last = (xb == p.W - 1);

@@ -138,6 +138,7 @@ hs_status run_passes_dev(const float *Ix, const float *Iy, const float *It, int 
         pp.H = H; pp.W = W; pp.ld = ld;
         pp.alpha2 = alpha2;
         pp.alpha_dev = alpha_dev;
+        pp.dump = 0;
         pp.we = rc.we; pp.wc = rc.wc;
         const int sc = strip_cols_for(t);
         pp.nstrips = (W + sc - 1) / sc;

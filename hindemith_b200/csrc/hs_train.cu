@@ -1,0 +1,744 @@
+// hs_train.cu -- batched differentiable Horn-Schunck: forward with checkpoints and the
+// temporally blocked adjoint, for n pairs per launch.
+//
+// Forward.  The sweeps run interval by interval (ckpt_every sweeps each): every pass is
+// one table-driven launch over all pairs; an interval's first pass reads checkpoint b and
+// its last pass writes checkpoint b+1, so checkpoints cost no copies.
+//
+// Backward, interval by interval in reverse:
+//  1. Recompute the interval's states x_{k+1} with "dump" passes of the forward kernel:
+//     every stage of a pass also writes its sweep, so T states cost one pass.
+//  2. Adjoint passes of TB sweeps each.  Because the clamp-to-edge average is symmetric
+//     in each axis, its transpose is itself (A^T = A), so the adjoint of a sweep is
+//     "pointwise map M, then A": with lambda = dL/dx_{k+1},
+//         g = Ix lu + Iy lv, lr = -g/d, z = lambda + lr (Ix, Iy), lambda_k = A z,
+//     and the gradient accumulations of sweep k need ubar, vbar, t of sweep k, which follow
+//     pointwise from x_{k+1}:  t = (Ix u_{k+1} + Iy v_{k+1} + It) / alpha^2,
+//     ubar = u_{k+1} + Ix t, vbar = v_{k+1} + Iy t  (d t = r and r - (Ix^2+Iy^2) t = alpha^2 t).
+//     The adjoint pass is therefore the forward's register pipeline with M in place of
+//     the Jacobi update: stage 0 applies M to the incoming lambda row, stage s applies A
+//     and then M of the next sweep; per-row accumulators live in a shared-memory ring
+//     beside the coefficients and are added to HBM once per pass.
+//  3. Transposed derivative stencils and the alpha reduction, per pair.
+// The gradient needs alpha != 0 (t is recovered through 1/alpha^2).
+#include <algorithm>
+#include <vector>
+
+#include "hs_stream.cuh"
+
+namespace hs {
+
+constexpr int kMaxTrainPairs = 32;
+constexpr int kMaxTB = 5;
+
+// ------------------------------------------------------------------ table-driven pass
+
+struct PassTable {
+    SweepParams pair[kMaxTrainPairs];
+    int item_prefix[kMaxTrainPairs + 1];
+    int npairs;
+};
+
+__device__ __forceinline__ int find_pair(const int *prefix, int n, int item) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= item) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+template <int T, bool FAST>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3 : 2)))
+    hs_table_pass_kernel(const __grid_constant__ PassTable tab) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * Geo<T>::warp_floats;
+    griddep_launch_dependents();
+    griddep_wait();
+    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    if (item >= tab.item_prefix[tab.npairs]) return;
+    const int pi = find_pair(tab.item_prefix, tab.npairs, item);
+    const SweepParams &p = tab.pair[pi];
+    const int local = item - tab.item_prefix[pi];
+    Item it;
+    init_item<T>(it, p, local % p.nstrips, local / p.nstrips, lane, wbase);
+    run_item<T, FAST>(p, it);
+}
+
+template <int T, bool FAST>
+static hs_status launch_table(const PassTable &tab, cudaStream_t s) {
+    auto fn = hs_table_pass_kernel<T, FAST>;
+    static bool attr[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, Geo<T>::smem_bytes));
+        attr[dev] = true;
+    }
+    const int items = tab.item_prefix[tab.npairs];
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
+    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.dynamicSmemBytes = Geo<T>::smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, fn, tab));
+    return HS_OK;
+}
+
+static hs_status launch_table_any(int T, bool fast, const PassTable &tab, cudaStream_t s) {
+#define HS_CASE(TT) \
+    case TT: return fast ? launch_table<TT, true>(tab, s) : launch_table<TT, false>(tab, s);
+    switch (T) { HS_CASE(1) HS_CASE(2) HS_CASE(3) HS_CASE(4) HS_CASE(5) HS_CASE(6) HS_CASE(7) HS_CASE(8) }
+#undef HS_CASE
+    HS_FAIL(HS_ERR_INVALID_ARG, "pass depth %d outside 1..8", T);
+}
+
+// ------------------------------------------------------------------ adjoint pass
+
+struct AdjPair {
+    const float *Ix, *Iy, *It;
+    const float *lu_in, *lv_in;
+    float *lu_out, *lv_out;
+    const float *xu[kMaxTB], *xv[kMaxTB];  // x_{k_hi - s}, s = 0..TB-1
+    float *aIx, *aIy, *aIt, *aA2;          // accumulators (+=)
+    const float *alpha_dev;
+    int H, W, ld, seg_rows, nstrips;
+};
+
+struct AdjTable {
+    AdjPair pair[kMaxTrainPairs];
+    int item_prefix[kMaxTrainPairs + 1];
+    int npairs;
+    float we, wc;
+};
+
+template <int TB>
+struct AdjGeo {
+    static constexpr int coef_slots = TB + 1;
+    static constexpr int raw_floats = kRawSlots * kRawPlanes * kWarpCols;
+    static constexpr int ring_floats = coef_slots * 2 * 2 * 32 * 4;  // [slot][coef|acc][col][lane] float4
+    static constexpr int warp_floats = raw_floats + ring_floats;
+    static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
+};
+
+// M of one sweep at one column: lambda (lu, lv) -> z, adding this sweep's gradient terms to
+// acc (aIx, aIy, aIt, aA2).  C = (Ix, Iy, It, 1/d); (xu, xv) = x_{k+1}.
+__device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, float xu, float xv,
+                                          float inv_a2, float &zu, float &zv, float4 &acc) {
+    const float g = fmaf(C.x, lu, C.y * lv);
+    const float lr = -g * C.w;
+    zu = fmaf(lr, C.x, lu);
+    zv = fmaf(lr, C.y, lv);
+    const float t = fmaf(C.x, xu, fmaf(C.y, xv, C.z)) * inv_a2;
+    const float ub = fmaf(C.x, t, xu), vb = fmaf(C.y, t, xv);
+    const float ld = g * t * C.w;
+    acc.x = fmaf(-lu, t, fmaf(lr, ub, fmaf(2.f * C.x, ld, acc.x)));
+    acc.y = fmaf(-lv, t, fmaf(lr, vb, fmaf(2.f * C.y, ld, acc.y)));
+    acc.z += lr;
+    acc.w += ld;
+}
+
+template <int TB, bool XEDGE, bool EDGE>
+__device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp, const Item &it,
+                                         float4 *ring, Win<true> (&w)[TB][2][2], float inv_a2,
+                                         float we, float wc, int k, int rslot, int cslot) {
+    __syncwarp();
+    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
+    // state rows of every stage (pointwise), issued before waiting on the ring
+    float2 xs[TB][2];
+#pragma unroll
+    for (int s = 0; s < TB; ++s) {
+        const int r = min(max(k - s, 0), P.H - 1);
+        const size_t off = (size_t)r * P.ld + it.lc2;
+        xs[s][0] = __ldg(reinterpret_cast<const float2 *>(P.xu[s] + off));
+        xs[s][1] = __ldg(reinterpret_cast<const float2 *>(P.xv[s] + off));
+    }
+    cp_async_wait<kPrefetch>();
+    __syncwarp();
+
+    // stage 0: lambda row k arrives; coefficients, zeroed accumulators, then M
+    const float *raw = it.raw + rslot * (kRawPlanes * kWarpCols) + 2 * it.lane;
+    const float2 l2u = lds2(raw), l2v = lds2(raw + kWarpCols);
+    float cu[2][2];
+    {
+        const float2 ix = lds2(raw + 2 * kWarpCols), iy = lds2(raw + 3 * kWarpCols);
+        const float2 t2 = lds2(raw + 4 * kWarpCols);
+        const float ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
+        const float ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
+        const float4 C[2] = {make_float4(ix.x, iy.x, t2.x, ax), make_float4(ix.y, iy.y, t2.y, ay)};
+        float4 *slot = ring + cslot * 128 + it.lane;
+        const float lu[2] = {l2u.x, l2u.y}, lv[2] = {l2v.x, l2v.y};
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float xu = j ? xs[0][0].y : xs[0][0].x, xv = j ? xs[0][1].y : xs[0][1].x;
+            adj_point(lu[j], lv[j], C[j], xu, xv, inv_a2, cu[0][j], cu[1][j], acc);
+            slot[32 * j] = C[j];
+            slot[64 + 32 * j] = acc;
+        }
+    }
+#pragma unroll
+    for (int s = 1; s <= TB; ++s) {
+        const int n = k - s + 1;  // arriving row
+        float lam[2][2];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const float ca = cu[q][0], cb = cu[q][1];
+            const float fromL = __shfl_up_sync(kFull, cb, 1);
+            const float fromR = __shfl_down_sync(kFull, ca, 1);
+            float la = fromL, ra = cb, rb = fromR;
+            if constexpr (XEDGE) {
+                la = it.a_first ? ca : la;
+                ra = it.a_last ? ca : ra;
+                rb = it.b_last ? cb : rb;
+            }
+            lam[q][0] = win_step<EDGE>(w[s - 1][q][0], la, ca, ra, n, P.H, we, wc);
+            lam[q][1] = win_step<EDGE>(w[s - 1][q][1], ca, cb, rb, n, P.H, we, wc);
+        }
+        if (s < TB) {  // M of the next sweep at row k - s
+            int rs = cslot - s;
+            if (rs < 0) rs += AdjGeo<TB>::coef_slots;
+            float4 *slot = ring + rs * 128 + it.lane;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const float4 C = slot[32 * j];
+                float4 acc = slot[64 + 32 * j];
+                const float xu = j ? xs[s][0].y : xs[s][0].x, xv = j ? xs[s][1].y : xs[s][1].x;
+                adj_point(lam[0][j], lam[1][j], C, xu, xv, inv_a2, cu[0][j], cu[1][j], acc);
+                slot[64 + 32 * j] = acc;
+            }
+        } else {
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) cu[q][j] = lam[q][j];
+        }
+    }
+
+    // flush the accumulators of row k - (TB-1): its last sweep's M ran in this step
+    {
+        const int r = k - (TB - 1);
+        if (r >= it.y_start && r < it.y_end) {
+            int rs = cslot - (TB - 1);
+            if (rs < 0) rs += AdjGeo<TB>::coef_slots;
+            const float4 *slot = ring + rs * 128 + it.lane;
+            const float4 A0 = slot[64], A1 = slot[96];
+            const size_t off = (size_t)r * P.ld + it.xa;
+            if (it.st_a && it.st_b) {
+                float2 *pix = reinterpret_cast<float2 *>(P.aIx + off);
+                float2 *piy = reinterpret_cast<float2 *>(P.aIy + off);
+                float2 *pit = reinterpret_cast<float2 *>(P.aIt + off);
+                float2 *pa2 = reinterpret_cast<float2 *>(P.aA2 + off);
+                float2 v;
+                v = *pix; v.x += A0.x; v.y += A1.x; *pix = v;
+                v = *piy; v.x += A0.y; v.y += A1.y; *piy = v;
+                v = *pit; v.x += A0.z; v.y += A1.z; *pit = v;
+                v = *pa2; v.x += A0.w; v.y += A1.w; *pa2 = v;
+            } else if (it.st_a) {
+                P.aIx[off] += A0.x;
+                P.aIy[off] += A0.y;
+                P.aIt[off] += A0.z;
+                P.aA2[off] += A0.w;
+            }
+        }
+    }
+    // store lambda_{k_hi - TB} of row k - TB
+    {
+        const int r = k - TB;
+        if (r >= it.y_start && r < it.y_end) {
+            const size_t off = (size_t)r * P.ld + it.xa;
+            if (it.st_a && it.st_b) {
+                *reinterpret_cast<float2 *>(P.lu_out + off) = make_float2(cu[0][0], cu[0][1]);
+                *reinterpret_cast<float2 *>(P.lv_out + off) = make_float2(cu[1][0], cu[1][1]);
+            } else if (it.st_a) {
+                P.lu_out[off] = cu[0][0];
+                P.lv_out[off] = cu[1][0];
+            }
+        }
+    }
+}
+
+template <int TB, bool XEDGE>
+__device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp, const Item &it,
+                                         float4 *ring, float we, float wc) {
+    const float a = __ldg(P.alpha_dev);
+    const float inv_a2 = 1.0f / (a * a);
+    const int k0 = max(0, it.y_start - TB);
+    const int k_end = it.y_end - 1 + TB;
+    Win<true> w[TB][2][2];
+#pragma unroll
+    for (int s = 0; s < TB; ++s)
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+#pragma unroll
+            for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
+#pragma unroll
+    for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, lp);
+    const int klo = max(k0, TB);
+    const int khi = min(k_end, P.H - 2);
+    int k = k0, rslot = 0, cslot = 0;
+    auto advance = [&]() {
+        ++k;
+        rslot = (rslot + 1) & (kRawSlots - 1);
+        cslot = (cslot + 1 == AdjGeo<TB>::coef_slots) ? 0 : cslot + 1;
+    };
+    if (klo + 1 <= khi) {
+        for (; k < klo; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+        while (k + 1 <= khi) {
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+            advance();
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+            advance();
+        }
+    }
+    for (; k <= k_end; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+    cp_async_wait<0>();
+}
+
+template <int TB>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, 3)
+    hs_adjoint_pass_kernel(const __grid_constant__ AdjTable tab) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * AdjGeo<TB>::warp_floats;
+    griddep_launch_dependents();
+    griddep_wait();
+    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    if (item >= tab.item_prefix[tab.npairs]) return;
+    const int pi = find_pair(tab.item_prefix, tab.npairs, item);
+    const AdjPair &P = tab.pair[pi];
+    const int local = item - tab.item_prefix[pi];
+    // the row loads of the streaming machinery read lambda where the forward reads (u, v)
+    SweepParams lp;
+    lp.Ix = P.Ix;
+    lp.Iy = P.Iy;
+    lp.It = P.It;
+    lp.u_in = P.lu_in;
+    lp.v_in = P.lv_in;
+    lp.H = P.H;
+    lp.W = P.W;
+    lp.ld = P.ld;
+    lp.seg_rows = P.seg_rows;
+    lp.nstrips = P.nstrips;
+    lp.alpha2 = 0.f;
+    lp.alpha_dev = P.alpha_dev;
+    lp.dump = 0;
+    Item it;
+    init_item<TB>(it, lp, local % P.nstrips, local / P.nstrips, lane, wbase);
+    it.coef = reinterpret_cast<float4 *>(wbase + AdjGeo<TB>::raw_floats);
+    const int x0 = it.xa - 2 * lane;
+    if (x0 <= 0 || x0 + kWarpCols >= P.W) adj_item<TB, true>(P, lp, it, it.coef, tab.we, tab.wc);
+    else adj_item<TB, false>(P, lp, it, it.coef, tab.we, tab.wc);
+}
+
+template <int TB>
+static hs_status launch_adj(const AdjTable &tab, cudaStream_t s) {
+    auto fn = hs_adjoint_pass_kernel<TB>;
+    static bool attr[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, AdjGeo<TB>::smem_bytes));
+        attr[dev] = true;
+    }
+    const int items = tab.item_prefix[tab.npairs];
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
+    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.dynamicSmemBytes = AdjGeo<TB>::smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, fn, tab));
+    return HS_OK;
+}
+
+static hs_status launch_adj_any(int TB, const AdjTable &tab, cudaStream_t s) {
+    switch (TB) {
+        case 1: return launch_adj<1>(tab, s);
+        case 2: return launch_adj<2>(tab, s);
+        case 3: return launch_adj<3>(tab, s);
+        case 4: return launch_adj<4>(tab, s);
+        case 5: return launch_adj<5>(tab, s);
+    }
+    HS_FAIL(HS_ERR_INVALID_ARG, "adjoint depth %d outside 1..%d", TB, kMaxTB);
+}
+
+// ------------------------------------------------------------------ per-pair finishing
+
+struct FinishTable {
+    const float *dIx[kMaxTrainPairs], *dIy[kMaxTrainPairs], *dIt[kMaxTrainPairs], *dA2[kMaxTrainPairs];
+    float *dI0[kMaxTrainPairs], *dI1[kMaxTrainPairs];
+    const float *alpha[kMaxTrainPairs];
+    float *dalpha[kMaxTrainPairs];
+    double *partials;  // [npairs][256]
+    int H[kMaxTrainPairs], W[kMaxTrainPairs], ld[kMaxTrainPairs];
+    int npairs;
+};
+
+__device__ __forceinline__ int tap_src(int p, int o, int n, int xs[2]) {
+    int c = 0;
+    const int x = p - o;
+    if (x >= 0 && x <= n - 1) xs[c++] = x;
+    if (o == 1 && p == n - 1 && x != n - 1) xs[c++] = n - 1;  // (n-1) + 1 clamps to n-1
+    return c;
+}
+
+// dI0 = Dx^T dIx + Dy^T dIy - Dt^T dIt; dI1 = ... + Dt^T dIt (taps (0,0) (1,0) (0,1) (1,1)).
+__global__ void __launch_bounds__(256) batch_derivs_adjoint_kernel(const __grid_constant__ FinishTable ft) {
+    const int i = blockIdx.z;
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (i >= ft.npairs || x >= ft.W[i] || y >= ft.H[i]) return;
+    const int H = ft.H[i], W = ft.W[i], ld = ft.ld[i];
+    const float wx[4] = {-0.25f, 0.25f, -0.25f, 0.25f};
+    const float wy[4] = {-0.25f, -0.25f, 0.25f, 0.25f};
+    const int ox[4] = {0, 1, 0, 1}, oy[4] = {0, 0, 1, 1};
+    float sc = 0.f, st = 0.f;
+    for (int d = 0; d < 4; ++d) {
+        int xs[2], ys[2];
+        const int nx = tap_src(x, ox[d], W, xs), ny = tap_src(y, oy[d], H, ys);
+        for (int jy = 0; jy < ny; ++jy)
+            for (int jx = 0; jx < nx; ++jx) {
+                const size_t q = (size_t)ys[jy] * ld + xs[jx];
+                sc = fmaf(wx[d], __ldg(ft.dIx[i] + q), fmaf(wy[d], __ldg(ft.dIy[i] + q), sc));
+                st = fmaf(0.25f, __ldg(ft.dIt[i] + q), st);
+            }
+    }
+    const size_t o = (size_t)y * ld + x;
+    ft.dI0[i][o] = sc - st;
+    ft.dI1[i][o] = sc + st;
+}
+
+__global__ void __launch_bounds__(256) batch_sum_kernel(const __grid_constant__ FinishTable ft) {
+    __shared__ double sh[256];
+    const int i = blockIdx.y;
+    const int H = ft.H[i], W = ft.W[i], ld = ft.ld[i];
+    double s = 0.0;
+    const long n = (long)H * W;
+    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        s += (double)ft.dA2[i][(e / W) * ld + (e % W)];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) ft.partials[i * gridDim.x + blockIdx.x] = sh[0];
+}
+
+__global__ void __launch_bounds__(256) batch_fold_kernel(const __grid_constant__ FinishTable ft, int nparts) {
+    __shared__ double sh[256];
+    const int i = blockIdx.x;
+    double s = 0.0;
+    for (int e = threadIdx.x; e < nparts; e += blockDim.x) s += ft.partials[i * nparts + e];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *ft.dalpha[i] = (float)(2.0 * (double)__ldg(ft.alpha[i]) * sh[0]);
+}
+
+// ------------------------------------------------------------------ host plan
+
+constexpr int kSumBlocks = 128;
+
+struct TrainLayout {
+    size_t pb;            // plane stride (bytes)
+    size_t per_pair;      // bytes per pair
+    int nb;               // checkpoint intervals
+    int nstates;          // states kept for one interval (ckpt_every - 1)
+    // plane indices inside a pair's block
+    size_t derivs, ckpt, states, lam, acc, scratch;
+    size_t partials_off;  // after all pairs
+    size_t total;
+};
+
+static hs_status train_layout(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                              TrainLayout &L) {
+    if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
+    if (n < 1 || n > kMaxTrainPairs) HS_FAIL(HS_ERR_INVALID_ARG, "n=%d outside 1..%d", n, kMaxTrainPairs);
+    if (iters < 1 || ckpt_every < 1)
+        HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d must be >= 1", iters, ckpt_every);
+    size_t pbmax = 0;
+    for (int i = 0; i < n; ++i) {
+        hs_status st = check_plane_geometry(pairs[i].H, pairs[i].W, pairs[i].ld);
+        if (st != HS_OK) return st;
+        if (pairs[i].reserved != 0) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: reserved must be zero", i);
+        pbmax = std::max(pbmax, round_up(plane_bytes(pairs[i].H, pairs[i].ld), 256));
+    }
+    L.pb = pbmax;
+    L.nb = (iters + ckpt_every - 1) / ckpt_every;
+    L.nstates = ckpt_every - 1;
+    L.derivs = 0;                              // 3 planes
+    L.ckpt = 3;                                // (nb + 1) x 2 planes
+    L.states = L.ckpt + 2 * (size_t)(L.nb + 1);  // nstates x 2 planes
+    L.lam = L.states + 2 * (size_t)L.nstates;  // 2 x 2 planes
+    L.acc = L.lam + 4;                         // 4 planes
+    L.scratch = L.acc + 4;                     // 2 x 2 planes
+    L.per_pair = (L.scratch + 4) * L.pb;
+    L.partials_off = (size_t)n * L.per_pair;
+    L.total = L.partials_off + (size_t)n * kSumBlocks * sizeof(double);
+    return HS_OK;
+}
+
+static inline float *plane_at(char *ws, const TrainLayout &L, int i, size_t idx) {
+    return reinterpret_cast<float *>(ws + (size_t)i * L.per_pair + idx * L.pb);
+}
+
+static SweepParams base_params(const hs_train_pair &d, const float *Ix, const float *Iy,
+                               const float *It, const ResolvedConfig &rc, int T) {
+    SweepParams p;
+    memset(&p, 0, sizeof(p));
+    p.Ix = Ix;
+    p.Iy = Iy;
+    p.It = It;
+    p.H = d.H;
+    p.W = d.W;
+    p.ld = d.ld;
+    p.alpha2 = 0.f;
+    p.alpha_dev = d.alpha;
+    p.we = rc.we;
+    p.wc = rc.wc;
+    const int sc = strip_cols_for(T);
+    p.nstrips = (d.W + sc - 1) / sc;
+    p.dump = 0;
+    return p;
+}
+
+// rows per work item for a table launch: about one wave of warps over all pairs
+static void set_segments(PassTable &tab, int T) {
+    long rows = 0;
+    for (int i = 0; i < tab.npairs; ++i) rows += (long)tab.pair[i].nstrips * tab.pair[i].H;
+    const long target = (long)sm_count() * 16;
+    int L = (int)std::max(1L, (rows + target - 1) / target);
+    L = std::max(L, 2 * T);
+    tab.item_prefix[0] = 0;
+    for (int i = 0; i < tab.npairs; ++i) {
+        SweepParams &p = tab.pair[i];
+        p.seg_rows = std::min(std::max(L, 8), p.H);
+        p.nitems = p.nstrips * ((p.H + p.seg_rows - 1) / p.seg_rows);
+        tab.item_prefix[i + 1] = tab.item_prefix[i] + p.nitems;
+    }
+}
+
+}  // namespace hs
+
+using namespace hs;
+
+extern "C" {
+
+size_t hs_train_workspace_bytes(const hs_train_pair *pairs, int n, int iters, int ckpt_every) {
+    TrainLayout L;
+    if (train_layout(pairs, n, iters, ckpt_every, L) != HS_OK) return 0;
+    return L.total;
+}
+
+hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                                   void *workspace, size_t workspace_bytes, const hs_config *cfg,
+                                   void *stream) {
+    clear_error();
+    TrainLayout L;
+    hs_status st = train_layout(pairs, n, iters, ckpt_every, L);
+    if (st != HS_OK) return st;
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
+    if (!workspace || workspace_bytes < L.total)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, L.total);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+        HS_FAIL(HS_ERR_ALIGNMENT, "workspace is not 256-byte aligned");
+    for (int i = 0; i < n; ++i) {
+        const void *pl[4] = {pairs[i].I0, pairs[i].I1, pairs[i].u, pairs[i].v};
+        const char *nm[4] = {"I0", "I1", "u", "v"};
+        for (int q = 0; q < 4; ++q)
+            if ((st = check_plane(pl[q], nm[q])) != HS_OK) return st;
+        if (!pairs[i].alpha) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: alpha (device) is NULL", i);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    char *ws = reinterpret_cast<char *>(workspace);
+    for (int i = 0; i < n; ++i) {
+        const hs_train_pair &d = pairs[i];
+        float *Ix = plane_at(ws, L, i, 0), *Iy = plane_at(ws, L, i, 1), *It = plane_at(ws, L, i, 2);
+        if ((st = hs_derivs(d.I0, d.I1, d.H, d.W, d.ld, Ix, Iy, It, stream)) != HS_OK) return st;
+        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.ckpt), 0, 2 * L.pb, s));  // x_0 = 0
+    }
+    const int T = rc.T;
+    for (int b = 0; b < L.nb; ++b) {
+        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
+        const int passes = (nsw + T - 1) / T;
+        for (int q = 0, done = 0; q < passes; ++q) {
+            const int t = std::min(T, nsw - done);
+            PassTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            for (int i = 0; i < n; ++i) {
+                SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
+                                            plane_at(ws, L, i, 2), rc, t);
+                const size_t in = q == 0 ? L.ckpt + 2 * b : L.scratch + 2 * ((q - 1) & 1);
+                const size_t out = q == passes - 1 ? L.ckpt + 2 * (b + 1) : L.scratch + 2 * (q & 1);
+                p.u_in = plane_at(ws, L, i, in);
+                p.v_in = plane_at(ws, L, i, in + 1);
+                p.u_out = plane_at(ws, L, i, out);
+                p.v_out = plane_at(ws, L, i, out + 1);
+                tab.pair[i] = p;
+            }
+            set_segments(tab, t);
+            if ((st = launch_table_any(t, rc.fast, tab, s)) != HS_OK) return st;
+            done += t;
+        }
+    }
+    for (int i = 0; i < n; ++i) {  // the final state is checkpoint nb; hand it out as (u, v)
+        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
+        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].u, plane_at(ws, L, i, L.ckpt + 2 * L.nb), pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].v, plane_at(ws, L, i, L.ckpt + 2 * L.nb + 1), pl, cudaMemcpyDeviceToDevice, s));
+    }
+    return HS_OK;
+}
+
+hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                              void *workspace, size_t workspace_bytes, const hs_config *cfg,
+                              void *stream) {
+    clear_error();
+    TrainLayout L;
+    hs_status st = train_layout(pairs, n, iters, ckpt_every, L);
+    if (st != HS_OK) return st;
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
+    if (!workspace || workspace_bytes < L.total)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, L.total);
+    for (int i = 0; i < n; ++i) {
+        const void *pl[4] = {pairs[i].dLdu, pairs[i].dLdv, pairs[i].dI0, pairs[i].dI1};
+        const char *nm[4] = {"dLdu", "dLdv", "dI0", "dI1"};
+        for (int q = 0; q < 4; ++q)
+            if ((st = check_plane(pl[q], nm[q])) != HS_OK) return st;
+        if (!pairs[i].alpha || !pairs[i].dalpha)
+            HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: alpha / dalpha (device) NULL", i);
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    char *ws = reinterpret_cast<char *>(workspace);
+    for (int i = 0; i < n; ++i) {
+        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
+        HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam), pairs[i].dLdu, pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam + 1), pairs[i].dLdv, pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.acc), 0, 4 * L.pb, s));
+    }
+    int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
+    const int TB = std::min(kMaxTB, std::max(1, rc.T));
+    for (int b = L.nb - 1; b >= 0; --b) {
+        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
+        // 1. states x_{k_lo+1} .. x_{k_lo+nsw-1} into states[0..nsw-2]
+        for (int done = 0; done < nsw - 1;) {
+            const int t = std::min(5, nsw - 1 - done);  // dump depth: 9 states = 5 + 4
+            PassTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            for (int i = 0; i < n; ++i) {
+                SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
+                                            plane_at(ws, L, i, 2), rc, t);
+                const size_t in = done == 0 ? L.ckpt + 2 * b : L.states + 2 * (done - 1);
+                p.u_in = plane_at(ws, L, i, in);
+                p.v_in = plane_at(ws, L, i, in + 1);
+                p.dump = 1;
+                for (int q = 0; q < t; ++q) {
+                    p.dump_u[q] = plane_at(ws, L, i, L.states + 2 * (done + q));
+                    p.dump_v[q] = plane_at(ws, L, i, L.states + 2 * (done + q) + 1);
+                }
+                p.u_out = p.dump_u[t - 1];
+                p.v_out = p.dump_v[t - 1];
+                tab.pair[i] = p;
+            }
+            set_segments(tab, t);
+            if ((st = launch_table_any(t, rc.fast, tab, s)) != HS_OK) return st;
+            done += t;
+        }
+        // 2. adjoint sweeps j = nsw-1 .. 0 in passes of up to TB
+        for (int jhi = nsw; jhi > 0;) {
+            const int tb = std::min(TB, jhi);
+            AdjTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            tab.we = rc.we;
+            tab.wc = rc.wc;
+            long rows = 0;
+            for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
+            int Lr = (int)std::max(1L, (rows + (long)sm_count() * 12 - 1) / ((long)sm_count() * 12));
+            Lr = std::max(Lr, std::max(8, 2 * tb));
+            tab.item_prefix[0] = 0;
+            for (int i = 0; i < n; ++i) {
+                const hs_train_pair &d = pairs[i];
+                AdjPair &P = tab.pair[i];
+                P.Ix = plane_at(ws, L, i, 0);
+                P.Iy = plane_at(ws, L, i, 1);
+                P.It = plane_at(ws, L, i, 2);
+                P.lu_in = plane_at(ws, L, i, L.lam + 2 * cur);
+                P.lv_in = plane_at(ws, L, i, L.lam + 2 * cur + 1);
+                P.lu_out = plane_at(ws, L, i, L.lam + 2 * (cur ^ 1));
+                P.lv_out = plane_at(ws, L, i, L.lam + 2 * (cur ^ 1) + 1);
+                for (int q = 0; q < tb; ++q) {
+                    const int j = jhi - q;  // x_{k_lo + j}
+                    const size_t idx = (j == nsw) ? L.ckpt + 2 * (b + 1) : L.states + 2 * (j - 1);
+                    P.xu[q] = plane_at(ws, L, i, idx);
+                    P.xv[q] = plane_at(ws, L, i, idx + 1);
+                }
+                P.aIx = plane_at(ws, L, i, L.acc);
+                P.aIy = plane_at(ws, L, i, L.acc + 1);
+                P.aIt = plane_at(ws, L, i, L.acc + 2);
+                P.aA2 = plane_at(ws, L, i, L.acc + 3);
+                P.alpha_dev = d.alpha;
+                P.H = d.H;
+                P.W = d.W;
+                P.ld = d.ld;
+                P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
+                P.seg_rows = std::min(Lr, d.H);
+                tab.item_prefix[i + 1] = tab.item_prefix[i] + P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
+            }
+            if ((st = launch_adj_any(tb, tab, s)) != HS_OK) return st;
+            cur ^= 1;
+            jhi -= tb;
+        }
+    }
+    // 3. transposed derivative stencils and dalpha
+    FinishTable ft;
+    memset(&ft, 0, sizeof(ft));
+    ft.npairs = n;
+    ft.partials = reinterpret_cast<double *>(ws + L.partials_off);
+    int maxW = 1, maxH = 1;
+    for (int i = 0; i < n; ++i) {
+        ft.dIx[i] = plane_at(ws, L, i, L.acc);
+        ft.dIy[i] = plane_at(ws, L, i, L.acc + 1);
+        ft.dIt[i] = plane_at(ws, L, i, L.acc + 2);
+        ft.dA2[i] = plane_at(ws, L, i, L.acc + 3);
+        ft.dI0[i] = pairs[i].dI0;
+        ft.dI1[i] = pairs[i].dI1;
+        ft.alpha[i] = pairs[i].alpha;
+        ft.dalpha[i] = pairs[i].dalpha;
+        ft.H[i] = pairs[i].H;
+        ft.W[i] = pairs[i].W;
+        ft.ld[i] = pairs[i].ld;
+        maxW = std::max(maxW, pairs[i].W);
+        maxH = std::max(maxH, pairs[i].H);
+    }
+    batch_derivs_adjoint_kernel<<<dim3((maxW + 63) / 64, (maxH + 3) / 4, n), dim3(64, 4), 0, s>>>(ft);
+    HS_LAUNCH_CHECK("batch_derivs_adjoint_kernel");
+    batch_sum_kernel<<<dim3(kSumBlocks, n), 256, 0, s>>>(ft);
+    HS_LAUNCH_CHECK("batch_sum_kernel");
+    batch_fold_kernel<<<n, 256, 0, s>>>(ft, kSumBlocks);
+    HS_LAUNCH_CHECK("batch_fold_kernel");
+    return HS_OK;
+}
+
+}  // extern "C"

@@ -188,6 +188,38 @@ HS_API hs_status hs_backward(const float *derivs, int H, int W, int ld, const fl
                              void *workspace, size_t workspace_bytes, const hs_config *cfg,
                              void *stream);
 
+/* n pairs (1..32) of one differentiable batch; all device pointers.  The forward reads
+ * I0, I1, alpha and writes u, v; the backward reads dLdu, dLdv, alpha and writes dI0,
+ * dI1 and dalpha (one float). */
+typedef struct hs_train_pair {
+    const float *I0, *I1;
+    float *u, *v;
+    const float *alpha;
+    const float *dLdu, *dLdv;
+    float *dI0, *dI1;
+    float *dalpha;
+    int H, W, ld;
+    int reserved; /* must be zero */
+} hs_train_pair;
+
+/* Workspace shared by hs_forward_train_batched and the matching hs_backward_batched
+ * (derivatives, checkpoints, one interval's states, adjoint buffers per pair). */
+HS_API size_t hs_train_workspace_bytes(const hs_train_pair *pairs, int n, int iters, int ckpt_every);
+
+/* Forward of n pairs with checkpoints every ckpt_every sweeps kept in the workspace; each
+ * pass is one launch over all pairs.  Results equal hs_forward per pair. */
+HS_API hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int iters,
+                                          int ckpt_every, void *workspace, size_t workspace_bytes,
+                                          const hs_config *cfg, void *stream);
+
+/* Backward of the preceding hs_forward_train_batched (same pairs, iters, ckpt_every and
+ * workspace): per checkpoint interval, the states are recomputed by dump passes (each
+ * stage of a T-sweep pass writes its state) and the adjoint runs temporally blocked,
+ * sweeps_per_pass (at most 5) adjoint sweeps per HBM pass.  Needs alpha != 0. */
+HS_API hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                                     void *workspace, size_t workspace_bytes,
+                                     const hs_config *cfg, void *stream);
+
 /* ---- allocation-free forward ------------------------------------------------- */
 
 /* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for

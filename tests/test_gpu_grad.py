@@ -142,3 +142,78 @@ def test_grad_fast_form(cuda):
                                      lam_u, lam_v)
     assert rel_err(g0, r0) < REL and rel_err(g1, r1) < REL
     assert abs(ga - ra) <= REL * abs(ra)
+
+
+# ---------------------------------------------------------------- batched training path
+
+def run_batch_grad(imgs, alpha, iters, lams, ckpt_every=10, T=4, fast=True):
+    from hindemith_b200.autograd import horn_schunck_batch
+
+    a = torch.tensor(alpha, dtype=torch.float32, device="cuda", requires_grad=True)
+    xs = [(cuda32(I0).requires_grad_(True), cuda32(I1).requires_grad_(True)) for I0, I1 in imgs]
+    outs = horn_schunck_batch(xs, a, iters, ckpt_every, L.make_config(sweeps_per_pass=T, fast_math=fast))
+    loss = 0
+    for (u, v), (lu, lv) in zip(outs, lams):
+        loss = loss + (u * cuda32(lu)).sum() + (v * cuda32(lv)).sum()
+    loss.backward()
+    torch.cuda.synchronize()
+    return ([(x0.grad.cpu().numpy(), x1.grad.cpu().numpy()) for x0, x1 in xs], float(a.grad),
+            [(u.detach().cpu().numpy(), v.detach().cpu().numpy()) for u, v in outs])
+
+
+@pytest.mark.parametrize("T", [1, 3, 4, 5])
+@pytest.mark.parametrize("ckpt", [1, 7, 10])
+def test_batched_grad_matches_fp64_adjoint(cuda, T, ckpt):
+    shapes = [(24, 31), (33, 65), (1, 9), (70, 130)]
+    iters, alpha = 23, 0.8
+    rng = np.random.default_rng(T * 10 + ckpt)
+    imgs = [synthetic.make_pair(H, W, seed=500 + i)[:2] for i, (H, W) in enumerate(shapes)]
+    lams = [(rng.standard_normal(s), rng.standard_normal(s)) for s in shapes]
+    grads, ga, outs = run_batch_grad(imgs, alpha, iters, lams, ckpt, T)
+    ra_total = 0.0
+    for (I0, I1), (lu, lv), (g0, g1), (u, v) in zip(imgs, lams, grads, outs):
+        r0, r1, ra, (ru, rv) = O.hs_adjoint_f64(I0.astype(np.float64), I1.astype(np.float64),
+                                                alpha, iters, lu, lv)
+        ra_total += ra
+        assert rel_err(g0, r0) < REL and rel_err(g1, r1) < REL
+        assert np.abs(u - ru).max() < 1e-4
+    assert abs(ga - ra_total) <= REL * abs(ra_total)
+
+
+def test_batched_train_forward_equals_forward(cuda):
+    from hindemith_b200.autograd import horn_schunck_batch
+
+    imgs = [synthetic.make_pair(H, W, seed=9 + H)[:2] for H, W in ((64, 80), (17, 23))]
+    a = torch.tensor(1.2, device="cuda")
+    cfg = L.make_config(sweeps_per_pass=4)
+    outs = horn_schunck_batch([(cuda32(x), cuda32(y)) for x, y in imgs], a, 37, 10, cfg)
+    for (u, v), (I0, I1) in zip(outs, imgs):
+        ru, rv = D.hs_forward(D.as_plane(cuda32(I0)), D.as_plane(cuda32(I1)), 1.2, 37, cfg)
+        torch.cuda.synchronize()
+        assert_bitexact(u.cpu().numpy(), ru.cpu().numpy(), "u")
+        assert_bitexact(v.cpu().numpy(), rv.cpu().numpy(), "v")
+
+
+def test_batched_grad_epe_config3_crop(cuda):
+    """Four 64x64 crops, 200 sweeps, checkpoints every 10, mean EPE: against torch float64."""
+    from hindemith_b200.autograd import horn_schunck_batch
+
+    data = [synthetic.make_pair(64, 64, seed=1000 + i) for i in range(4)]
+    a = torch.tensor(1.0, device="cuda", requires_grad=True)
+    xs = [(cuda32(d[0]).requires_grad_(True), cuda32(d[1]).requires_grad_(True)) for d in data]
+    outs = horn_schunck_batch(xs, a, 200, 10, L.make_config(sweeps_per_pass=4, fast_math=True))
+    loss = sum(mean_epe(u, v, cuda32(d[2]), cuda32(d[3])) for (u, v), d in zip(outs, data)) / 4
+    loss.backward()
+    ta = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    tx = [(torch.from_numpy(d[0].astype(np.float64)).requires_grad_(True),
+           torch.from_numpy(d[1].astype(np.float64)).requires_grad_(True)) for d in data]
+    tl = 0
+    for (t0, t1), d in zip(tx, data):
+        ru, rv = hs_torch(t0, t1, ta, 200)
+        tl = tl + mean_epe(ru, rv, torch.from_numpy(d[2].astype(np.float64)),
+                           torch.from_numpy(d[3].astype(np.float64)))
+    (tl / 4).backward()
+    for (x0, x1), (t0, t1) in zip(xs, tx):
+        assert rel_err(x0.grad.cpu().numpy(), t0.grad.numpy()) < REL
+        assert rel_err(x1.grad.cpu().numpy(), t1.grad.numpy()) < REL
+    assert abs(float(a.grad) - float(ta.grad)) <= REL * abs(float(ta.grad))
