@@ -46,6 +46,11 @@ def parse_args():
     ap.add_argument("--shape", default="", help="HxW override (profiling cases)")
     ap.add_argument("--iters", type=int, default=0, help="sweep count override")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-pairs", type=int, default=64,
+                    help="pairs of the mixed batch (a prefix of the 64-pair list)")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-train", action="store_true")
+    ap.add_argument("--train-sweeps-per-pass", type=int, default=4)
     return ap.parse_args()
 
 
@@ -173,6 +178,128 @@ def run_reference(args, rank, world):
                        "sample_sweeps_per_step": sweeps},
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+
+# ------------------------------------------------------------------ extra workloads
+
+def timed_events(fn, k, warmup, flush, stream, label):
+    """Sum of K per-step CUDA-event durations (s); L2 flushed between steps."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+        flush.zero_()
+    torch.cuda.synchronize()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(k)]
+    torch.cuda.nvtx.range_push(label)
+    for a, b in evs:
+        a.record(stream)
+        fn()
+        b.record(stream)
+        flush.zero_()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in evs) / 1e3
+
+
+def measure_batched(args, rank, flush, peak):
+    """The mixed batch (64 pairs, 320x240 .. 2048x2048, alpha in [0.5, 2], 100/200/500
+    sweeps): one graph-captured persistent launch, against one plain hs_forward per pair."""
+    import torch
+
+    from hindemith_b200 import _lib as L
+    from hindemith_b200 import device as D
+    from hindemith_b200 import synthetic
+    from hindemith_b200.batched import BatchPlan
+
+    specs = synthetic.batch_mixed()[: args.batch_pairs]
+    for sp in specs:
+        sp.seed += 100 * rank
+    T = 4
+    cfg = L.make_config(sweeps_per_pass=T, fast_math=not args.exact)
+    plan = BatchPlan([(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs], cfg)
+    for i, sp in enumerate(specs):
+        I0, I1, _, _ = synthetic.generate(sp)
+        plan.I0[i].copy_(torch.from_numpy(I0))
+        plan.I1[i].copy_(torch.from_numpy(I1))
+    plan.capture()
+    stream = torch.cuda.current_stream()
+    t_b = timed_events(plan.replay, args.steps, 3, flush, stream, "timed_batched")
+    plan.check()
+    outs = [D.empty_planes(2, sp.H, sp.W) for sp in specs]
+
+    def plain():
+        for i, sp in enumerate(specs):
+            D.hs_forward(plan.I0[i], plan.I1[i], sp.alpha, sp.iters, cfg, out=(outs[i][0], outs[i][1]))
+
+    t_p = timed_events(plain, max(1, args.steps // 4), 1, flush, stream, "timed_plain_loop")
+    same = all(torch.equal(plan.u[i], outs[i][0]) and torch.equal(plan.v[i], outs[i][1])
+               for i in range(len(specs)))
+    px_it = plan.pixel_iters
+    passes = sum(sp.H * sp.W * ((sp.iters + T - 1) // T) for sp in specs)
+    achieved = BYTES_PER_PX_PASS * passes * args.steps / t_b / 1e9
+    return {
+        "workload": f"hs_batched_{len(specs)}pairs_mixed", "pairs": len(specs),
+        "mpix": round(sum(sp.H * sp.W for sp in specs) / 1e6, 3), "pix_iters": px_it,
+        "sweeps_per_pass": T, "launch": "one persistent kernel per batch, CUDA graph replay",
+        "value": px_it * args.steps / t_b / 1e6, "unit": UNIT,
+        "ms_per_step": t_b / args.steps * 1e3,
+        "plain_loop": {"value": px_it * max(1, args.steps // 4) / t_p / 1e6,
+                       "ms_per_step": t_p / max(1, args.steps // 4) * 1e3,
+                       "launch": "one hs_forward call per pair"},
+        "identical_to_plain": bool(same),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "bytes_per_px_pass": BYTES_PER_PX_PASS},
+    }
+
+
+def measure_train(args, rank, flush):
+    """Differentiable workload: 16 pairs of 512x512, 200 sweeps, alpha learnable (1.0),
+    mean end-point error to the synthetic flow, checkpoints every 10 sweeps; the batched
+    training API (one launch per pass for all pairs)."""
+    import torch
+
+    from hindemith_b200 import _lib as L
+    from hindemith_b200 import device as D
+    from hindemith_b200 import synthetic
+    from hindemith_b200.autograd import horn_schunck_batch
+
+    specs = synthetic.batch_512(16)
+    data = []
+    for sp in specs:
+        sp.seed += 100 * rank
+        I0, I1, ut, vt = synthetic.generate(sp)
+        data.append(tuple(D.as_plane(torch.from_numpy(a).cuda()) for a in (I0, I1, ut, vt)))
+    T = args.train_sweeps_per_pass
+    cfg = L.make_config(sweeps_per_pass=T, fast_math=not args.exact)
+    alpha = torch.tensor(1.0, device="cuda", requires_grad=True)
+
+    def fwd():
+        with torch.no_grad():
+            horn_schunck_batch([(d[0], d[1]) for d in data], alpha, 200, 10, cfg)
+
+    def fwd_bwd():
+        alpha.grad = None
+        xs = [(d[0].detach().requires_grad_(True), d[1].detach().requires_grad_(True)) for d in data]
+        outs = horn_schunck_batch(xs, alpha, 200, 10, cfg)
+        loss = 0.0
+        for (u, v), d in zip(outs, data):
+            loss = loss + torch.sqrt((u - d[2]) ** 2 + (v - d[3]) ** 2 + 1e-12).mean()
+        (loss / len(data)).backward()
+
+    stream = torch.cuda.current_stream()
+    k = max(1, args.steps // 4)
+    t_f = timed_events(fwd, k, 3, flush, stream, "timed_train_fwd")
+    t_fb = timed_events(fwd_bwd, k, 3, flush, stream, "timed_train_fwd_bwd")
+    px_it = sum(sp.H * sp.W * sp.iters for sp in specs)
+    return {"workload": "hs_train_16x512x512_200sweeps_ckpt10", "pix_iters": px_it,
+            "sweeps_per_pass": T, "api": "horn_schunck_batch (hs_forward_train_batched + hs_backward_batched)",
+            "fwd_ms": t_f / k * 1e3, "fwd_bwd_ms": t_fb / k * 1e3,
+            "fwd_bwd_over_fwd": t_fb / t_f,
+            "fwd_value": px_it * k / t_f / 1e6,
+            "value": px_it * k / t_fb / 1e6, "unit": UNIT + " (forward+backward)"}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -326,6 +453,11 @@ def main():
         "gpu_launches": (1 + passes) * args.steps,
         "clocks": clocks,
     }
+    # the batched and differentiable workloads are single-GPU measurements
+    if world == 1 and not args.no_batched and not args.shape:
+        line["batched"] = measure_batched(args, rank, flush, peak)
+    if world == 1 and not args.no_train and not args.shape:
+        line["fwd_bwd"] = measure_train(args, rank, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(I0h, I1h, alpha, args.cpu_sample_sweeps)
     if rank == 0:

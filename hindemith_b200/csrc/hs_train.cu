@@ -146,14 +146,11 @@ __device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, f
     acc.w += ld;
 }
 
-template <int TB, bool XEDGE, bool EDGE>
-__device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp, const Item &it,
-                                         float4 *ring, Win<true> (&w)[TB][2][2], float inv_a2,
-                                         float we, float wc, int k, int rslot, int cslot) {
-    __syncwarp();
-    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
-    // state rows of every stage (pointwise), issued before waiting on the ring
-    float2 xs[TB][2];
+// Global loads one step ahead: the state rows every stage uses at step k, and the
+// accumulator values of the row flushed at step k.
+template <int TB>
+__device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, int k,
+                                             float2 (&xs)[TB][2], float2 (&accp)[4]) {
 #pragma unroll
     for (int s = 0; s < TB; ++s) {
         const int r = min(max(k - s, 0), P.H - 1);
@@ -161,6 +158,21 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
         xs[s][0] = __ldg(reinterpret_cast<const float2 *>(P.xu[s] + off));
         xs[s][1] = __ldg(reinterpret_cast<const float2 *>(P.xv[s] + off));
     }
+    const int r = min(max(k - (TB - 1), 0), P.H - 1);
+    const size_t off = (size_t)r * P.ld + (it.st_a ? it.xa : it.lc2);
+    accp[0] = *reinterpret_cast<const float2 *>(P.aIx + off);
+    accp[1] = *reinterpret_cast<const float2 *>(P.aIy + off);
+    accp[2] = *reinterpret_cast<const float2 *>(P.aIt + off);
+    accp[3] = *reinterpret_cast<const float2 *>(P.aA2 + off);
+}
+
+template <int TB, bool XEDGE, bool EDGE>
+__device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp, const Item &it,
+                                         float4 *ring, Win<true> (&w)[TB][2][2], float inv_a2,
+                                         float we, float wc, int k, int rslot, int cslot,
+                                         float2 (&xs)[TB][2], float2 (&accp)[4]) {
+    __syncwarp();
+    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
     cp_async_wait<kPrefetch>();
     __syncwarp();
 
@@ -233,23 +245,19 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
             const float4 A0 = slot[64], A1 = slot[96];
             const size_t off = (size_t)r * P.ld + it.xa;
             if (it.st_a && it.st_b) {
-                float2 *pix = reinterpret_cast<float2 *>(P.aIx + off);
-                float2 *piy = reinterpret_cast<float2 *>(P.aIy + off);
-                float2 *pit = reinterpret_cast<float2 *>(P.aIt + off);
-                float2 *pa2 = reinterpret_cast<float2 *>(P.aA2 + off);
-                float2 v;
-                v = *pix; v.x += A0.x; v.y += A1.x; *pix = v;
-                v = *piy; v.x += A0.y; v.y += A1.y; *piy = v;
-                v = *pit; v.x += A0.z; v.y += A1.z; *pit = v;
-                v = *pa2; v.x += A0.w; v.y += A1.w; *pa2 = v;
+                *reinterpret_cast<float2 *>(P.aIx + off) = make_float2(accp[0].x + A0.x, accp[0].y + A1.x);
+                *reinterpret_cast<float2 *>(P.aIy + off) = make_float2(accp[1].x + A0.y, accp[1].y + A1.y);
+                *reinterpret_cast<float2 *>(P.aIt + off) = make_float2(accp[2].x + A0.z, accp[2].y + A1.z);
+                *reinterpret_cast<float2 *>(P.aA2 + off) = make_float2(accp[3].x + A0.w, accp[3].y + A1.w);
             } else if (it.st_a) {
-                P.aIx[off] += A0.x;
-                P.aIy[off] += A0.y;
-                P.aIt[off] += A0.z;
-                P.aA2[off] += A0.w;
+                P.aIx[off] = accp[0].x + A0.x;
+                P.aIy[off] = accp[1].x + A0.y;
+                P.aIt[off] = accp[2].x + A0.z;
+                P.aA2[off] = accp[3].x + A0.w;
             }
         }
     }
+    adj_prefetch<TB>(P, it, k + 1, xs, accp);  // for the next step
     // store lambda_{k_hi - TB} of row k - TB
     {
         const int r = k - TB;
@@ -282,6 +290,8 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
             for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
 #pragma unroll
     for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, lp);
+    float2 xs[TB][2], accp[4];
+    adj_prefetch<TB>(P, it, k0, xs, accp);
     const int klo = max(k0, TB);
     const int khi = min(k_end, P.H - 2);
     int k = k0, rslot = 0, cslot = 0;
@@ -291,15 +301,15 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
         cslot = (cslot + 1 == AdjGeo<TB>::coef_slots) ? 0 : cslot + 1;
     };
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+        for (; k < klo; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
         while (k + 1 <= khi) {
-            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
             advance();
-            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
             advance();
         }
     }
-    for (; k <= k_end; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot);
+    for (; k <= k_end; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
     cp_async_wait<0>();
 }
 
