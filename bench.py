@@ -51,6 +51,8 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--train-sweeps-per-pass", type=int, default=4)
+    ap.add_argument("--no-pyramid", action="store_true")
+    ap.add_argument("--pyramid-pairs", type=int, default=8)
     return ap.parse_args()
 
 
@@ -302,6 +304,78 @@ def measure_train(args, rank, flush):
             "value": px_it * k / t_fb / 1e6, "unit": UNIT + " (forward+backward)"}
 
 
+def measure_pyramid(args, rank, flush):
+    """Coarse-to-fine workload: 8 pairs of 2048x2048 with flow up to 12 px, 4 levels
+    (binomial blur + decimation), warp of I1 by the upsampled flow at each finer level,
+    100 sweeps per level checkpointed every 10, loss = mean end-point error; forward and
+    backward through all levels captured in ONE CUDA graph and replayed."""
+    import torch
+
+    from hindemith_b200 import _lib as L
+    from hindemith_b200 import device as D
+    from hindemith_b200 import synthetic
+    from hindemith_b200.pyramid import coarse_to_fine
+
+    specs = synthetic.batch_pyramid(args.pyramid_pairs)
+    levels, iters = 4, 100
+    data = []
+    for sp in specs:
+        sp.seed += 100 * rank
+        I0, I1, ut, vt = synthetic.generate(sp)
+        data.append(tuple(D.as_plane(torch.from_numpy(a).cuda()) for a in (I0, I1, ut, vt)))
+    cfg = L.make_config(sweeps_per_pass=args.train_sweeps_per_pass, fast_math=not args.exact)
+    alpha0 = torch.tensor(1.0, device="cuda")
+
+    def fwd_bwd():
+        # fresh leaves per call: an autograd leaf remembers the stream it was first used on
+        alpha = alpha0.detach().requires_grad_(True)
+        xs = [(d[0].detach().requires_grad_(True), d[1].detach().requires_grad_(True))
+              for d in data]
+        flows = coarse_to_fine(xs, alpha, levels, iters, 10, cfg)
+        loss = 0.0
+        for (u, v), d in zip(flows, data):
+            loss = loss + torch.sqrt((u - d[2]) ** 2 + (v - d[3]) ** 2 + 1e-12).mean()
+        loss = loss / len(data)
+        return (loss, *torch.autograd.grad(loss, [alpha] + [t for p in xs for t in p]))
+
+    torch.cuda.synchronize()
+    base = torch.cuda.memory_allocated()
+    torch.cuda.reset_peak_memory_stats()
+    eager = fwd_bwd()
+    torch.cuda.synchronize()
+    eager_peak = torch.cuda.max_memory_allocated() - base
+    del eager
+    stream = torch.cuda.current_stream()
+    k = max(1, args.steps // 4)
+    t_eager = timed_events(fwd_bwd, k, 1, flush, stream, "timed_pyramid_eager")
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        fwd_bwd()
+    stream.wait_stream(side)
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        outs = fwd_bwd()
+    torch.cuda.synchronize()
+    graph_peak = torch.cuda.max_memory_allocated() - base
+    t_graph = timed_events(graph.replay, k, 3, flush, stream, "timed_pyramid_graph")
+    loss = float(outs[0].detach())
+    px_it = sum(sum(((sp.H + (1 << l) - 1) >> l) * ((sp.W + (1 << l) - 1) >> l)
+                    for l in range(levels)) * iters for sp in specs)
+    del outs, graph
+    return {"workload": f"hs_pyramid_{len(specs)}x2048x2048_4levels_100sweeps_ckpt10",
+            "pix_iters_fwd": px_it, "sweeps_per_pass": args.train_sweeps_per_pass,
+            "api": "pyramid.coarse_to_fine (hs_blur_down, hs_upsample2, hs_warp, batched HS) "
+                   "+ torch.autograd.grad, one CUDA graph",
+            "fwd_bwd_ms": t_graph / k * 1e3, "fwd_bwd_eager_ms": t_eager / k * 1e3,
+            "value": px_it * k / t_graph / 1e6, "unit": UNIT + " (forward+backward, all levels)",
+            "loss": loss, "peak_device_bytes": int(max(eager_peak, graph_peak)),
+            "peak_device_bytes_eager": int(eager_peak), "peak_device_bytes_graph": int(graph_peak),
+            "input_bytes": int(base)}
+
+
 # ------------------------------------------------------------------ GPU arm
 
 def main():
@@ -458,6 +532,8 @@ def main():
         line["batched"] = measure_batched(args, rank, flush, peak)
     if world == 1 and not args.no_train and not args.shape:
         line["fwd_bwd"] = measure_train(args, rank, flush)
+    if world == 1 and not args.no_pyramid and not args.shape:
+        line["pyramid"] = measure_pyramid(args, rank, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(I0h, I1h, alpha, args.cpu_sample_sweeps)
     if rank == 0:

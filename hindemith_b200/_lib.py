@@ -111,6 +111,12 @@ SIGNATURES = {
     "hs_train_workspace_bytes": (_sz, [_tpp, _i, _i, _i]),
     "hs_forward_train_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
+    "hs_blur_down": (_i, [_vp, _i, _i, _i, _vp, _i, _vp]),
+    "hs_blur_down_adjoint": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
+    "hs_upsample2": (_i, [_vp, _i, _vp, _i, _i, _i, _f, _vp]),
+    "hs_upsample2_adjoint": (_i, [_vp, _i, _i, _i, _vp, _i, _f, _vp]),
+    "hs_warp": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
+    "hs_warp_adjoint": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
     "hs_backward": (_i, [_vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
                          _cfgp, _vp]),
 }

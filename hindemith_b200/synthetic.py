@@ -115,5 +115,11 @@ def batch_512(n: int = 16) -> List[PairSpec]:
     return [PairSpec(i, 512, 512, 1.0, 200, 1000 + i) for i in range(n)]
 
 
+def batch_pyramid(n: int = 8) -> List[PairSpec]:
+    """n 2048x2048 pairs with large flow (up to 12 px), alpha 1, 100 sweeps per level (the
+    coarse-to-fine workload)."""
+    return [PairSpec(i, 2048, 2048, 1.0, 100, 3000 + i, sigma=2.0, amplitude=12.0) for i in range(n)]
+
+
 def generate(spec: PairSpec):
     return make_pair(spec.H, spec.W, spec.seed, spec.sigma, spec.amplitude)

@@ -220,6 +220,36 @@ HS_API hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iter
                                      void *workspace, size_t workspace_bytes,
                                      const hs_config *cfg, void *stream);
 
+/* ---- coarse-to-fine pieces ---------------------------------------------------- */
+
+/* out = every second pixel of the 5x5 binomial blur ([1 4 6 4 1]/16 per axis, clamp-to-edge
+ * taps) of in: out is ceil(H/2) x ceil(W/2) with row stride ldo.  The reference builds
+ * pyramids from Stencil2DMVM (Stencil2DMVM.cpp:34-59); this fuses the blur and the
+ * decimation.  The adjoint overwrites din (H x W, stride ld) with the transpose applied
+ * to dout. */
+HS_API hs_status hs_blur_down(const float *in, int H, int W, int ld, float *out, int ldo, void *stream);
+HS_API hs_status hs_blur_down_adjoint(const float *dout, int H, int W, int ld, int ldo, float *din,
+                                      void *stream);
+
+/* fine (H x W) = scale * 2x bilinear upsampling of coarse (ceil(H/2) x ceil(W/2), stride
+ * ldc), half-pixel centres, clamped coarse indices (scale = 2 for a flow field).  No
+ * counterpart in the reference.  The adjoint overwrites dcoarse. */
+HS_API hs_status hs_upsample2(const float *coarse, int ldc, float *fine, int H, int W, int ld,
+                              float scale, void *stream);
+HS_API hs_status hs_upsample2_adjoint(const float *dfine, int H, int W, int ld, float *dcoarse,
+                                      int ldc, float scale, void *stream);
+
+/* dst = src backward-warped by the offsets (u, v) with WarpImg2D's semantics
+ * (Operations/OpticalFlow/WarpImg2D.cpp:33-75): bilinear when the 2x2 footprint at
+ * (x + u, y + v) lies inside the image, else the source pixel; bit-identical to the
+ * template's float/double arithmetic.  The adjoint adds dL/dsrc into dsrc (atomic scatter)
+ * and overwrites du, dv with dL/du, dL/dv (piecewise derivative). */
+HS_API hs_status hs_warp(const float *src, const float *u, const float *v, int H, int W, int ld,
+                         float *dst, void *stream);
+HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *v,
+                                 const float *ddst, int H, int W, int ld, float *dsrc, float *du,
+                                 float *dv, void *stream);
+
 /* ---- allocation-free forward ------------------------------------------------- */
 
 /* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for

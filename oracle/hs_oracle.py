@@ -315,3 +315,116 @@ def hs_adjoint_f64(I0, I1, alpha, iters, lam_u, lam_v):
     dI1 = dxT(DX_W, dIx) + dxT(DY_W, dIy) + dxT(DT_W, dIt)
     return dI0, dI1, 2.0 * f64(alpha) * da2, (u, v)
 
+
+
+# ---------------------------------------------------------------- pyramid pieces (FP64)
+
+BINOMIAL5 = np.array([1.0, 4.0, 6.0, 4.0, 1.0]) / 16.0
+
+
+def blur_down(x):
+    """5x5 binomial blur (separable [1 4 6 4 1]/16, clamp-to-edge taps), then keep every
+    second pixel: out[y, x] = blur(x)[2y, 2x], shape (ceil(H/2), ceil(W/2))."""
+    x = np.asarray(x, np.float64)
+    H, W = x.shape
+    Ho, Wo = (H + 1) // 2, (W + 1) // 2
+    out = np.zeros((Ho, Wo))
+    for dy in range(-2, 3):
+        rr = np.clip(2 * np.arange(Ho) + dy, 0, H - 1)
+        for dx in range(-2, 3):
+            cc = np.clip(2 * np.arange(Wo) + dx, 0, W - 1)
+            out += BINOMIAL5[dy + 2] * BINOMIAL5[dx + 2] * x[rr][:, cc]
+    return out
+
+
+def blur_down_adjoint(g, H, W):
+    g = np.asarray(g, np.float64)
+    Ho, Wo = g.shape
+    out = np.zeros((H, W))
+    for dy in range(-2, 3):
+        rr = np.clip(2 * np.arange(Ho) + dy, 0, H - 1)
+        for dx in range(-2, 3):
+            cc = np.clip(2 * np.arange(Wo) + dx, 0, W - 1)
+            np.add.at(out, (rr[:, None], cc[None, :]), BINOMIAL5[dy + 2] * BINOMIAL5[dx + 2] * g)
+    return out
+
+
+def _up_axis(n_fine, n_coarse):
+    """Per fine index: (i0, i1, f) of the 2x bilinear upsampling with half-pixel centres
+    (source coordinate (i + 0.5)/2 - 0.5), indices clamped into the coarse axis."""
+    c = (np.arange(n_fine) + 0.5) / 2.0 - 0.5
+    i0 = np.floor(c).astype(np.int64)
+    f = c - i0
+    return np.clip(i0, 0, n_coarse - 1), np.clip(i0 + 1, 0, n_coarse - 1), f
+
+
+def upsample2(c, H, W, scale=2.0):
+    """(H, W) = scale * bilinear 2x upsampling of c (Hc, Wc) with Hc = ceil(H/2)."""
+    c = np.asarray(c, np.float64)
+    Hc, Wc = c.shape
+    y0, y1, fy = _up_axis(H, Hc)
+    x0, x1, fx = _up_axis(W, Wc)
+    fy, fx = fy[:, None], fx[None, :]
+    return scale * ((1 - fy) * ((1 - fx) * c[y0][:, x0] + fx * c[y0][:, x1])
+                    + fy * ((1 - fx) * c[y1][:, x0] + fx * c[y1][:, x1]))
+
+
+def upsample2_adjoint(g, Hc, Wc, scale=2.0):
+    g = np.asarray(g, np.float64)
+    H, W = g.shape
+    y0, y1, fy = _up_axis(H, Hc)
+    x0, x1, fx = _up_axis(W, Wc)
+    out = np.zeros((Hc, Wc))
+    for yi, wy in ((y0, 1 - fy), (y1, fy)):
+        for xi, wx in ((x0, 1 - fx), (x1, fx)):
+            np.add.at(out, (yi[:, None], xi[None, :]), scale * wy[:, None] * wx[None, :] * g)
+    return out
+
+
+def warp_f64(src, ox, oy):
+    """WarpImg2D.cpp:33-75 in exact FP64 arithmetic (no float roundings)."""
+    src = np.asarray(src, np.float64)
+    ox = np.asarray(ox, np.float64)
+    oy = np.asarray(oy, np.float64)
+    H, W = src.shape
+    mx = np.floor(ox).astype(np.int64)
+    my = np.floor(oy).astype(np.int64)
+    xf, yf = ox - mx, oy - my
+    Y, X = np.mgrid[0:H, 0:W]
+    ok = (X + mx >= 0) & (X + mx + 1 < W) & (Y + my >= 0) & (Y + my + 1 < H)
+    bx = np.where(ok, X + mx, 0)
+    by = np.where(ok, Y + my, 0)
+    bx1 = np.minimum(bx + 1, W - 1)
+    by1 = np.minimum(by + 1, H - 1)
+    o = (src[by, bx] * (1 - xf) * (1 - yf) + src[by, bx1] * xf * (1 - yf)
+         + src[by1, bx] * (1 - xf) * yf + src[by1, bx1] * xf * yf)
+    return np.where(ok, o, src)
+
+
+def warp_adjoint_f64(src, ox, oy, g):
+    """(dsrc, dox, doy) of <g, warp(src, ox, oy)> (piecewise derivative; the integer part
+    and the in-bounds test are locally constant)."""
+    src = np.asarray(src, np.float64)
+    ox = np.asarray(ox, np.float64)
+    oy = np.asarray(oy, np.float64)
+    g = np.asarray(g, np.float64)
+    H, W = src.shape
+    mx = np.floor(ox).astype(np.int64)
+    my = np.floor(oy).astype(np.int64)
+    xf, yf = ox - mx, oy - my
+    Y, X = np.mgrid[0:H, 0:W]
+    ok = (X + mx >= 0) & (X + mx + 1 < W) & (Y + my >= 0) & (Y + my + 1 < H)
+    bx = np.where(ok, X + mx, 0)
+    by = np.where(ok, Y + my, 0)
+    bx1 = np.minimum(bx + 1, W - 1)
+    by1 = np.minimum(by + 1, H - 1)
+    dsrc = np.zeros((H, W))
+    go = np.where(ok, g, 0.0)
+    for yy, xx, w in ((by, bx, (1 - xf) * (1 - yf)), (by, bx1, xf * (1 - yf)),
+                      (by1, bx, (1 - xf) * yf), (by1, bx1, xf * yf)):
+        np.add.at(dsrc, (yy, xx), w * go)
+    dsrc += np.where(ok, 0.0, g)
+    s00, s10, s01, s11 = src[by, bx], src[by, bx1], src[by1, bx], src[by1, bx1]
+    dox = go * ((1 - yf) * (s10 - s00) + yf * (s11 - s01))
+    doy = go * ((1 - xf) * (s01 - s00) + xf * (s11 - s10))
+    return dsrc, dox, doy

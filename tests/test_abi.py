@@ -129,3 +129,18 @@ def test_batched_workspace_and_argument_checks():
     arr[1].reserved = 0
     arr[0].iters = -1
     assert lib.hs_forward_batched(arr, 2, p, nb, ctypes.byref(cfg), None, None) == L.HS_ERR_INVALID_ARG
+
+
+def test_pyramid_argument_checks():
+    lib = L.lib()
+    P, Q = fake_ptr(), fake_ptr(256)
+    # coarse stride below ceil(W/2), unaligned stride, null and unaligned planes, aliasing
+    assert lib.hs_blur_down(P, 8, 8, 8, Q, 2, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_blur_down(P, 8, 6, 6, Q, 4, None) == L.HS_ERR_ALIGNMENT
+    assert lib.hs_blur_down(None, 8, 8, 8, Q, 4, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_blur_down_adjoint(P, 0, 8, 8, 4, Q, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_upsample2(P, 2, Q, 8, 8, 8, 2.0, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_upsample2_adjoint(P, 8, 8, 8, fake_ptr(4), 4, 2.0, None) == L.HS_ERR_ALIGNMENT
+    assert lib.hs_warp(P, P, P, 8, 8, 8, P, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_warp(P, P, None, 8, 8, 8, Q, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_warp_adjoint(P, P, P, P, 8, 7, 7, Q, Q, Q, None) == L.HS_ERR_ALIGNMENT

@@ -139,3 +139,52 @@ def test_torch_reference_matches_fp64_oracle():
     np.testing.assert_allclose(t0.grad.numpy(), r0, atol=1e-10)
     np.testing.assert_allclose(t1.grad.numpy(), r1, atol=1e-10)
     assert abs(float(ta.grad) - ra) < 1e-9
+
+
+def test_pyramid_adjoints_dot_product():
+    """<A x, y> = <x, A^T y> for blur-down and 2x upsampling; FD for the warp offsets."""
+    rng = np.random.default_rng(21)
+    for H, W in ((1, 1), (2, 3), (5, 8), (9, 7), (16, 16)):
+        x = rng.standard_normal((H, W))
+        y = rng.standard_normal(((H + 1) // 2, (W + 1) // 2))
+        assert abs((O.blur_down(x) * y).sum() - (x * O.blur_down_adjoint(y, H, W)).sum()) < 1e-12
+        c = rng.standard_normal(((H + 1) // 2, (W + 1) // 2))
+        z = rng.standard_normal((H, W))
+        assert abs((O.upsample2(c, H, W) * z).sum()
+                   - (c * O.upsample2_adjoint(z, c.shape[0], c.shape[1])).sum()) < 1e-12
+    H, W = 12, 15
+    src = rng.random((H, W))
+    ox = rng.uniform(-3, 3, (H, W))
+    oy = rng.uniform(-3, 3, (H, W))
+    g = rng.standard_normal((H, W))
+    dsrc, dox, doy = O.warp_adjoint_f64(src, ox, oy, g)
+    s2 = rng.standard_normal((H, W))
+    assert abs((O.warp_f64(s2, ox, oy) * g).sum() - (s2 * dsrc).sum()) < 1e-12
+    h = 1e-6
+    for i, j in ((3, 4), (6, 7), (10, 2)):
+        for arr, d in ((ox, dox), (oy, doy)):
+            p, m = arr.copy(), arr.copy()
+            p[i, j] += h
+            m[i, j] -= h
+            fp = O.warp_f64(src, p, oy) if arr is ox else O.warp_f64(src, ox, p)
+            fm = O.warp_f64(src, m, oy) if arr is ox else O.warp_f64(src, ox, m)
+            fd = ((fp - fm) * g).sum() / (2 * h)
+            assert abs(fd - d[i, j]) < 1e-6
+    # the FP64 warp agrees with the FP32-rounding restatement to float precision
+    assert np.abs(O.warp_f64(src, ox, oy) - O.warp(src, ox, oy)).max() < 1e-6
+
+
+def test_torch_pyramid_reference_matches_oracle():
+    import torch
+    from hs_torch_ref import blur_down_torch, upsample2_torch, warp_torch
+
+    rng = np.random.default_rng(17)
+    for H, W in [(1, 1), (5, 4), (37, 53)]:
+        x = rng.standard_normal((H, W))
+        c = O.blur_down(x)
+        assert np.array_equal(blur_down_torch(torch.tensor(x)).numpy(), c)
+        np.testing.assert_allclose(upsample2_torch(torch.tensor(c), H, W).numpy(),
+                                   O.upsample2(c, H, W), rtol=0, atol=1e-14)
+        ox, oy = rng.uniform(-3, 3, (H, W)), rng.uniform(-3, 3, (H, W))
+        np.testing.assert_allclose(warp_torch(torch.tensor(x), torch.tensor(ox), torch.tensor(oy)).numpy(),
+                                   O.warp_f64(x, ox, oy), rtol=0, atol=1e-14)
