@@ -267,6 +267,7 @@ def measure_train(args, rank, flush):
     from hindemith_b200 import device as D
     from hindemith_b200 import synthetic
     from hindemith_b200.autograd import horn_schunck_batch
+    from hindemith_b200.loss import mean_epe_batch
 
     specs = synthetic.batch_512(16)
     data = []
@@ -286,10 +287,7 @@ def measure_train(args, rank, flush):
         alpha.grad = None
         xs = [(d[0].detach().requires_grad_(True), d[1].detach().requires_grad_(True)) for d in data]
         outs = horn_schunck_batch(xs, alpha, 200, 10, cfg)
-        loss = 0.0
-        for (u, v), d in zip(outs, data):
-            loss = loss + torch.sqrt((u - d[2]) ** 2 + (v - d[3]) ** 2 + 1e-12).mean()
-        (loss / len(data)).backward()
+        mean_epe_batch(outs, [(d[2], d[3]) for d in data]).backward()
 
     stream = torch.cuda.current_stream()
     k = max(1, args.steps // 4)
@@ -297,7 +295,7 @@ def measure_train(args, rank, flush):
     t_fb = timed_events(fwd_bwd, k, 3, flush, stream, "timed_train_fwd_bwd")
     px_it = sum(sp.H * sp.W * sp.iters for sp in specs)
     return {"workload": "hs_train_16x512x512_200sweeps_ckpt10", "pix_iters": px_it,
-            "sweeps_per_pass": T, "api": "horn_schunck_batch (hs_forward_train_batched + hs_backward_batched)",
+            "sweeps_per_pass": T, "api": "horn_schunck_batch (hs_forward_train_batched + hs_backward_batched) + mean_epe_batch",
             "fwd_ms": t_f / k * 1e3, "fwd_bwd_ms": t_fb / k * 1e3,
             "fwd_bwd_over_fwd": t_fb / t_f,
             "fwd_value": px_it * k / t_f / 1e6,
@@ -314,6 +312,7 @@ def measure_pyramid(args, rank, flush):
     from hindemith_b200 import _lib as L
     from hindemith_b200 import device as D
     from hindemith_b200 import synthetic
+    from hindemith_b200.loss import mean_epe_batch
     from hindemith_b200.pyramid import coarse_to_fine
 
     specs = synthetic.batch_pyramid(args.pyramid_pairs)
@@ -332,10 +331,7 @@ def measure_pyramid(args, rank, flush):
         xs = [(d[0].detach().requires_grad_(True), d[1].detach().requires_grad_(True))
               for d in data]
         flows = coarse_to_fine(xs, alpha, levels, iters, 10, cfg)
-        loss = 0.0
-        for (u, v), d in zip(flows, data):
-            loss = loss + torch.sqrt((u - d[2]) ** 2 + (v - d[3]) ** 2 + 1e-12).mean()
-        loss = loss / len(data)
+        loss = mean_epe_batch(flows, [(d[2], d[3]) for d in data])
         return (loss, *torch.autograd.grad(loss, [alpha] + [t for p in xs for t in p]))
 
     torch.cuda.synchronize()

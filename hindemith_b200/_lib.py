@@ -61,6 +61,13 @@ class hs_pair_desc(ctypes.Structure):
 HS_MAX_BATCH = 128
 
 
+class hs_epe_pair(ctypes.Structure):
+    _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("ut", ctypes.c_void_p),
+                ("vt", ctypes.c_void_p), ("du", ctypes.c_void_p), ("dv", ctypes.c_void_p),
+                ("H", ctypes.c_int), ("W", ctypes.c_int), ("ld", ctypes.c_int),
+                ("reserved", ctypes.c_int)]
+
+
 class hs_train_pair(ctypes.Structure):
     _fields_ = [("I0", ctypes.c_void_p), ("I1", ctypes.c_void_p), ("u", ctypes.c_void_p),
                 ("v", ctypes.c_void_p), ("alpha", ctypes.c_void_p), ("dLdu", ctypes.c_void_p),
@@ -83,6 +90,7 @@ _fp = ctypes.POINTER(ctypes.c_float)
 _cfgp = ctypes.POINTER(hs_config)
 _pdp = ctypes.POINTER(hs_pair_desc)
 _tpp = ctypes.POINTER(hs_train_pair)
+_epp = ctypes.POINTER(hs_epe_pair)
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -111,6 +119,9 @@ SIGNATURES = {
     "hs_train_workspace_bytes": (_sz, [_tpp, _i, _i, _i]),
     "hs_forward_train_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
+    "hs_epe_workspace_bytes": (_sz, [_i]),
+    "hs_epe_loss_batched": (_i, [_epp, _i, _f, _vp, _vp, _sz, _vp]),
+    "hs_epe_loss_backward_batched": (_i, [_epp, _i, _f, _vp, _vp]),
     "hs_blur_down": (_i, [_vp, _i, _i, _i, _vp, _i, _vp]),
     "hs_blur_down_adjoint": (_i, [_vp, _i, _i, _i, _i, _vp, _vp]),
     "hs_upsample2": (_i, [_vp, _i, _vp, _i, _i, _i, _f, _vp]),

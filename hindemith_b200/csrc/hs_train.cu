@@ -30,6 +30,8 @@ namespace hs {
 
 constexpr int kMaxTrainPairs = 32;
 constexpr int kMaxTB = 5;
+constexpr int kAdjItemsPerSm = 12;  // adjoint work items (warps) per SM and launch
+constexpr int kMinStripCols = 48;   // narrowest strip: 64 columns less a halo of 8 each side
 
 // ------------------------------------------------------------------ table-driven pass
 
@@ -108,7 +110,8 @@ struct AdjPair {
     const float *lu_in, *lv_in;
     float *lu_out, *lv_out;
     const float *xu[kMaxTB], *xv[kMaxTB];  // x_{k_hi - s}, s = 0..TB-1
-    float *aIx, *aIy, *aIt, *aA2;          // accumulators (+=)
+    float *aIx, *aIy, *aIt;                // accumulators (+=, one owner per pixel per launch)
+    double *a2part;                        // per-item partial sums of dL/dalpha^2 (+=)
     const float *alpha_dev;
     int H, W, ld, seg_rows, nstrips;
 };
@@ -146,11 +149,10 @@ __device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, f
     acc.w += ld;
 }
 
-// Global loads one step ahead: the state rows every stage uses at step k, and the
-// accumulator values of the row flushed at step k.
+// Global loads one step ahead: the state rows every stage uses at step k.
 template <int TB>
 __device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, int k,
-                                             float2 (&xs)[TB][2], float2 (&accp)[4]) {
+                                             float2 (&xs)[TB][2]) {
 #pragma unroll
     for (int s = 0; s < TB; ++s) {
         const int r = min(max(k - s, 0), P.H - 1);
@@ -158,19 +160,13 @@ __device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, i
         xs[s][0] = __ldg(reinterpret_cast<const float2 *>(P.xu[s] + off));
         xs[s][1] = __ldg(reinterpret_cast<const float2 *>(P.xv[s] + off));
     }
-    const int r = min(max(k - (TB - 1), 0), P.H - 1);
-    const size_t off = (size_t)r * P.ld + (it.st_a ? it.xa : it.lc2);
-    accp[0] = *reinterpret_cast<const float2 *>(P.aIx + off);
-    accp[1] = *reinterpret_cast<const float2 *>(P.aIy + off);
-    accp[2] = *reinterpret_cast<const float2 *>(P.aIt + off);
-    accp[3] = *reinterpret_cast<const float2 *>(P.aA2 + off);
 }
 
 template <int TB, bool XEDGE, bool EDGE>
 __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp, const Item &it,
                                          float4 *ring, Win<true> (&w)[TB][2][2], float inv_a2,
                                          float we, float wc, int k, int rslot, int cslot,
-                                         float2 (&xs)[TB][2], float2 (&accp)[4]) {
+                                         float2 (&xs)[TB][2], float &a2s) {
     __syncwarp();
     issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
     cp_async_wait<kPrefetch>();
@@ -235,7 +231,9 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
         }
     }
 
-    // flush the accumulators of row k - (TB-1): its last sweep's M ran in this step
+    // flush the accumulators of row k - (TB-1): its last sweep's M ran in this step.  The
+    // adds are reductions performed in L2 (no value comes back to the warp); each pixel has
+    // one owner per launch and launches are stream-ordered, so the sums are deterministic.
     {
         const int r = k - (TB - 1);
         if (r >= it.y_start && r < it.y_end) {
@@ -245,19 +243,19 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
             const float4 A0 = slot[64], A1 = slot[96];
             const size_t off = (size_t)r * P.ld + it.xa;
             if (it.st_a && it.st_b) {
-                *reinterpret_cast<float2 *>(P.aIx + off) = make_float2(accp[0].x + A0.x, accp[0].y + A1.x);
-                *reinterpret_cast<float2 *>(P.aIy + off) = make_float2(accp[1].x + A0.y, accp[1].y + A1.y);
-                *reinterpret_cast<float2 *>(P.aIt + off) = make_float2(accp[2].x + A0.z, accp[2].y + A1.z);
-                *reinterpret_cast<float2 *>(P.aA2 + off) = make_float2(accp[3].x + A0.w, accp[3].y + A1.w);
+                atomicAdd(reinterpret_cast<float2 *>(P.aIx + off), make_float2(A0.x, A1.x));
+                atomicAdd(reinterpret_cast<float2 *>(P.aIy + off), make_float2(A0.y, A1.y));
+                atomicAdd(reinterpret_cast<float2 *>(P.aIt + off), make_float2(A0.z, A1.z));
+                a2s += A0.w + A1.w;
             } else if (it.st_a) {
-                P.aIx[off] = accp[0].x + A0.x;
-                P.aIy[off] = accp[1].x + A0.y;
-                P.aIt[off] = accp[2].x + A0.z;
-                P.aA2[off] = accp[3].x + A0.w;
+                atomicAdd(P.aIx + off, A0.x);
+                atomicAdd(P.aIy + off, A0.y);
+                atomicAdd(P.aIt + off, A0.z);
+                a2s += A0.w;
             }
         }
     }
-    adj_prefetch<TB>(P, it, k + 1, xs, accp);  // for the next step
+    adj_prefetch<TB>(P, it, k + 1, xs);  // for the next step
     // store lambda_{k_hi - TB} of row k - TB
     {
         const int r = k - TB;
@@ -276,7 +274,7 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
 
 template <int TB, bool XEDGE>
 __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp, const Item &it,
-                                         float4 *ring, float we, float wc) {
+                                         float4 *ring, float we, float wc, int local) {
     const float a = __ldg(P.alpha_dev);
     const float inv_a2 = 1.0f / (a * a);
     const int k0 = max(0, it.y_start - TB);
@@ -290,8 +288,9 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
             for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
 #pragma unroll
     for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, lp);
-    float2 xs[TB][2], accp[4];
-    adj_prefetch<TB>(P, it, k0, xs, accp);
+    float2 xs[TB][2];
+    float a2s = 0.f;
+    adj_prefetch<TB>(P, it, k0, xs);
     const int klo = max(k0, TB);
     const int khi = min(k_end, P.H - 2);
     int k = k0, rslot = 0, cslot = 0;
@@ -301,16 +300,21 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
         cslot = (cslot + 1 == AdjGeo<TB>::coef_slots) ? 0 : cslot + 1;
     };
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
+        for (; k < klo; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, a2s);
         while (k + 1 <= khi) {
-            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, a2s);
             advance();
-            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
+            adj_step<TB, XEDGE, false>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, a2s);
             advance();
         }
     }
-    for (; k <= k_end; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, accp);
+    for (; k <= k_end; advance()) adj_step<TB, XEDGE, true>(P, lp, it, ring, w, inv_a2, we, wc, k, rslot, cslot, xs, a2s);
     cp_async_wait<0>();
+    // this item's share of dL/dalpha^2: fixed-order butterfly, one owner per slot per launch
+    double d = (double)a2s;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d += __shfl_xor_sync(kFull, d, o);
+    if (it.lane == 0) P.a2part[local] += d;
 }
 
 template <int TB>
@@ -346,8 +350,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, 3)
     init_item<TB>(it, lp, local % P.nstrips, local / P.nstrips, lane, wbase);
     it.coef = reinterpret_cast<float4 *>(wbase + AdjGeo<TB>::raw_floats);
     const int x0 = it.xa - 2 * lane;
-    if (x0 <= 0 || x0 + kWarpCols >= P.W) adj_item<TB, true>(P, lp, it, it.coef, tab.we, tab.wc);
-    else adj_item<TB, false>(P, lp, it, it.coef, tab.we, tab.wc);
+    if (x0 <= 0 || x0 + kWarpCols >= P.W) adj_item<TB, true>(P, lp, it, it.coef, tab.we, tab.wc, local);
+    else adj_item<TB, false>(P, lp, it, it.coef, tab.we, tab.wc, local);
 }
 
 template <int TB>
@@ -389,11 +393,11 @@ static hs_status launch_adj_any(int TB, const AdjTable &tab, cudaStream_t s) {
 // ------------------------------------------------------------------ per-pair finishing
 
 struct FinishTable {
-    const float *dIx[kMaxTrainPairs], *dIy[kMaxTrainPairs], *dIt[kMaxTrainPairs], *dA2[kMaxTrainPairs];
+    const float *dIx[kMaxTrainPairs], *dIy[kMaxTrainPairs], *dIt[kMaxTrainPairs];
     float *dI0[kMaxTrainPairs], *dI1[kMaxTrainPairs];
     const float *alpha[kMaxTrainPairs];
     float *dalpha[kMaxTrainPairs];
-    double *partials;  // [npairs][256]
+    const double *a2part;  // [npairs][nslots]
     int H[kMaxTrainPairs], W[kMaxTrainPairs], ld[kMaxTrainPairs];
     int npairs;
 };
@@ -432,28 +436,11 @@ __global__ void __launch_bounds__(256) batch_derivs_adjoint_kernel(const __grid_
     ft.dI1[i][o] = sc + st;
 }
 
-__global__ void __launch_bounds__(256) batch_sum_kernel(const __grid_constant__ FinishTable ft) {
-    __shared__ double sh[256];
-    const int i = blockIdx.y;
-    const int H = ft.H[i], W = ft.W[i], ld = ft.ld[i];
-    double s = 0.0;
-    const long n = (long)H * W;
-    for (long e = (long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
-        s += (double)ft.dA2[i][(e / W) * ld + (e % W)];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) ft.partials[i * gridDim.x + blockIdx.x] = sh[0];
-}
-
 __global__ void __launch_bounds__(256) batch_fold_kernel(const __grid_constant__ FinishTable ft, int nparts) {
     __shared__ double sh[256];
     const int i = blockIdx.x;
     double s = 0.0;
-    for (int e = threadIdx.x; e < nparts; e += blockDim.x) s += ft.partials[i * nparts + e];
+    for (int e = threadIdx.x; e < nparts; e += blockDim.x) s += ft.a2part[(size_t)i * nparts + e];
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -465,7 +452,6 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const __grid_constant__
 
 // ------------------------------------------------------------------ host plan
 
-constexpr int kSumBlocks = 128;
 
 struct TrainLayout {
     size_t pb;            // plane stride (bytes)
@@ -474,7 +460,8 @@ struct TrainLayout {
     int nstates;          // states kept for one interval (ckpt_every - 1)
     // plane indices inside a pair's block
     size_t derivs, ckpt, states, lam, acc, scratch;
-    size_t partials_off;  // after all pairs
+    size_t partials_off;  // after all pairs: [n][nslots] doubles
+    int nslots;           // adjoint work items per pair and launch, upper bound
     size_t total;
 };
 
@@ -498,11 +485,15 @@ static hs_status train_layout(const hs_train_pair *pairs, int n, int iters, int 
     L.ckpt = 3;                                // (nb + 1) x 2 planes
     L.states = L.ckpt + 2 * (size_t)(L.nb + 1);  // nstates x 2 planes
     L.lam = L.states + 2 * (size_t)L.nstates;  // 2 x 2 planes
-    L.acc = L.lam + 4;                         // 4 planes
-    L.scratch = L.acc + 4;                     // 2 x 2 planes
+    L.acc = L.lam + 4;                         // 3 planes (dIx, dIy, dIt)
+    L.scratch = L.acc + 3;                     // 2 x 2 planes
     L.per_pair = (L.scratch + 4) * L.pb;
     L.partials_off = (size_t)n * L.per_pair;
-    L.total = L.partials_off + (size_t)n * kSumBlocks * sizeof(double);
+    // items of one pair in one adjoint launch <= (all rows / rows per item) + its strips
+    int maxW = 1;
+    for (int i = 0; i < n; ++i) maxW = std::max(maxW, pairs[i].W);
+    L.nslots = sm_count() * kAdjItemsPerSm + (maxW + kMinStripCols - 1) / kMinStripCols;
+    L.total = L.partials_off + round_up((size_t)n * L.nslots * sizeof(double), 256);
     return HS_OK;
 }
 
@@ -644,8 +635,9 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
         const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
         HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam), pairs[i].dLdu, pl, cudaMemcpyDeviceToDevice, s));
         HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam + 1), pairs[i].dLdv, pl, cudaMemcpyDeviceToDevice, s));
-        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.acc), 0, 4 * L.pb, s));
+        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.acc), 0, 3 * L.pb, s));
     }
+    HS_CUDA_CHECK(cudaMemsetAsync(ws + L.partials_off, 0, (size_t)n * L.nslots * sizeof(double), s));
     int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
     const int TB = std::min(kMaxTB, std::max(1, rc.T));
     for (int b = L.nb - 1; b >= 0; --b) {
@@ -685,7 +677,8 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
             tab.wc = rc.wc;
             long rows = 0;
             for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
-            int Lr = (int)std::max(1L, (rows + (long)sm_count() * 12 - 1) / ((long)sm_count() * 12));
+            const long target = (long)sm_count() * kAdjItemsPerSm;
+            int Lr = (int)std::max(1L, (rows + target - 1) / target);
             Lr = std::max(Lr, std::max(8, 2 * tb));
             tab.item_prefix[0] = 0;
             for (int i = 0; i < n; ++i) {
@@ -707,14 +700,16 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
                 P.aIx = plane_at(ws, L, i, L.acc);
                 P.aIy = plane_at(ws, L, i, L.acc + 1);
                 P.aIt = plane_at(ws, L, i, L.acc + 2);
-                P.aA2 = plane_at(ws, L, i, L.acc + 3);
+                P.a2part = reinterpret_cast<double *>(ws + L.partials_off) + (size_t)i * L.nslots;
                 P.alpha_dev = d.alpha;
                 P.H = d.H;
                 P.W = d.W;
                 P.ld = d.ld;
                 P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
                 P.seg_rows = std::min(Lr, d.H);
-                tab.item_prefix[i + 1] = tab.item_prefix[i] + P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
+                const int items = P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
+                if (items > L.nslots) HS_FAIL(HS_ERR_INVALID_ARG, "adjoint items %d > slots %d", items, L.nslots);
+                tab.item_prefix[i + 1] = tab.item_prefix[i] + items;
             }
             if ((st = launch_adj_any(tb, tab, s)) != HS_OK) return st;
             cur ^= 1;
@@ -725,13 +720,12 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
     FinishTable ft;
     memset(&ft, 0, sizeof(ft));
     ft.npairs = n;
-    ft.partials = reinterpret_cast<double *>(ws + L.partials_off);
+    ft.a2part = reinterpret_cast<const double *>(ws + L.partials_off);
     int maxW = 1, maxH = 1;
     for (int i = 0; i < n; ++i) {
         ft.dIx[i] = plane_at(ws, L, i, L.acc);
         ft.dIy[i] = plane_at(ws, L, i, L.acc + 1);
         ft.dIt[i] = plane_at(ws, L, i, L.acc + 2);
-        ft.dA2[i] = plane_at(ws, L, i, L.acc + 3);
         ft.dI0[i] = pairs[i].dI0;
         ft.dI1[i] = pairs[i].dI1;
         ft.alpha[i] = pairs[i].alpha;
@@ -744,9 +738,7 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
     }
     batch_derivs_adjoint_kernel<<<dim3((maxW + 63) / 64, (maxH + 3) / 4, n), dim3(64, 4), 0, s>>>(ft);
     HS_LAUNCH_CHECK("batch_derivs_adjoint_kernel");
-    batch_sum_kernel<<<dim3(kSumBlocks, n), 256, 0, s>>>(ft);
-    HS_LAUNCH_CHECK("batch_sum_kernel");
-    batch_fold_kernel<<<n, 256, 0, s>>>(ft, kSumBlocks);
+    batch_fold_kernel<<<n, 256, 0, s>>>(ft, L.nslots);
     HS_LAUNCH_CHECK("batch_fold_kernel");
     return HS_OK;
 }

@@ -250,6 +250,28 @@ HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *
                                  const float *ddst, int H, int W, int ld, float *dsrc, float *du,
                                  float *dv, void *stream);
 
+/* ---- loss ------------------------------------------------------------------- */
+
+/* One flow field and its target for the mean end-point-error loss; du, dv receive the
+ * gradient (backward only). */
+typedef struct hs_epe_pair {
+    const float *u, *v, *ut, *vt;
+    float *du, *dv;
+    int H, W, ld;
+    int reserved; /* must be zero */
+} hs_epe_pair;
+
+/* *loss (device float) = (1/n) sum_i mean_px sqrt((u-ut)^2 + (v-vt)^2 + eps) over n <= 32
+ * pairs, summed deterministically (double partials in a fixed order).  The reference's
+ * Array2DSum (Operations/DenseLinearAlgebra/Array2DSum.cpp:25-119) is its reduction
+ * building block; this fuses the pointwise error into the reduction.  The backward writes
+ * du, dv = dloss * (u-ut, v-vt) / (n H W sqrt(...)) with dloss a device float. */
+HS_API size_t hs_epe_workspace_bytes(int n);
+HS_API hs_status hs_epe_loss_batched(const hs_epe_pair *pairs, int n, float eps, float *loss,
+                                     void *workspace, size_t workspace_bytes, void *stream);
+HS_API hs_status hs_epe_loss_backward_batched(const hs_epe_pair *pairs, int n, float eps,
+                                              const float *dloss, void *stream);
+
 /* ---- allocation-free forward ------------------------------------------------- */
 
 /* Size of the library-owned scratch that hs_forward_noalloc uses: 48 MiB, enough for

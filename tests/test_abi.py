@@ -144,3 +144,24 @@ def test_pyramid_argument_checks():
     assert lib.hs_warp(P, P, P, 8, 8, 8, P, None) == L.HS_ERR_INVALID_ARG
     assert lib.hs_warp(P, P, None, 8, 8, 8, Q, None) == L.HS_ERR_INVALID_ARG
     assert lib.hs_warp_adjoint(P, P, P, P, 8, 7, 7, Q, Q, Q, None) == L.HS_ERR_ALIGNMENT
+
+
+def test_epe_argument_checks_before_launch():
+    lib = L.lib()
+    P = fake_ptr()
+    d = (L.hs_epe_pair * 2)()
+    for x in d:
+        x.u = x.v = x.ut = x.vt = 0x100000
+        x.H, x.W, x.ld = 4, 4, 4
+    assert lib.hs_epe_workspace_bytes(2) == 1024  # 2 x 64 doubles, rounded to 256
+    assert lib.hs_epe_loss_batched(d, 0, 0.0, P, P, 1024, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_epe_loss_batched(d, 2, -1.0, P, P, 1024, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_epe_loss_batched(d, 2, 0.0, P, P, 512, None) == L.HS_ERR_WORKSPACE
+    d[1].reserved = 1
+    assert lib.hs_epe_loss_batched(d, 2, 0.0, P, P, 1024, None) == L.HS_ERR_INVALID_ARG
+    d[1].reserved = 0
+    d[1].ld = 6
+    assert lib.hs_epe_loss_batched(d, 2, 0.0, P, P, 1024, None) == L.HS_ERR_ALIGNMENT
+    d[1].ld = 4
+    # the backward needs gradient planes
+    assert lib.hs_epe_loss_backward_batched(d, 2, 0.0, P, None) == L.HS_ERR_INVALID_ARG
