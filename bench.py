@@ -50,7 +50,7 @@ def parse_args():
                     help="pairs of the mixed batch (a prefix of the 64-pair list)")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-train", action="store_true")
-    ap.add_argument("--train-sweeps-per-pass", type=int, default=4)
+    ap.add_argument("--train-sweeps-per-pass", type=int, default=5)
     ap.add_argument("--no-pyramid", action="store_true")
     ap.add_argument("--pyramid-pairs", type=int, default=8)
     return ap.parse_args()
@@ -216,11 +216,14 @@ def measure_batched(args, rank, flush, peak):
     from hindemith_b200 import synthetic
     from hindemith_b200.batched import BatchPlan
 
+    from hindemith_b200.autotune import best_batch_config
+
     specs = synthetic.batch_mixed()[: args.batch_pairs]
     for sp in specs:
         sp.seed += 100 * rank
-    T = 4
-    cfg = L.make_config(sweeps_per_pass=T, fast_math=not args.exact)
+    shape = [(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs]
+    T, rows = best_batch_config(shape, fast_math=not args.exact)
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=rows, fast_math=not args.exact)
     plan = BatchPlan([(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs], cfg)
     for i, sp in enumerate(specs):
         I0, I1, _, _ = synthetic.generate(sp)
@@ -245,7 +248,8 @@ def measure_batched(args, rank, flush, peak):
     return {
         "workload": f"hs_batched_{len(specs)}pairs_mixed", "pairs": len(specs),
         "mpix": round(sum(sp.H * sp.W for sp in specs) / 1e6, 3), "pix_iters": px_it,
-        "sweeps_per_pass": T, "launch": "one persistent kernel per batch, CUDA graph replay",
+        "sweeps_per_pass": T, "rows_per_tile": rows, "autotuned": True,
+        "launch": "one persistent kernel per batch, CUDA graph replay",
         "value": px_it * args.steps / t_b / 1e6, "unit": UNIT,
         "ms_per_step": t_b / args.steps * 1e3,
         "plain_loop": {"value": px_it * max(1, args.steps // 4) / t_p / 1e6,

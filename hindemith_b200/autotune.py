@@ -2,9 +2,11 @@
 
 For an image shape it times candidate (T, rows_per_segment) pairs with CUDA events on
 the device (a fixed number of sweeps over synthetic coefficient planes of that shape)
-and keeps the fastest.  Results are cached per (device name, H, W, ld, mode) in memory
-and, when HS_AUTOTUNE_CACHE names a file, in that JSON file.  HS_AUTOTUNE_LOG names a
-file that receives every candidate's timing as one JSON line per tuning.
+and keeps the fastest; for a batch (`best_batch_config`) it times the persistent batched
+launch of that exact batch under each candidate (T, rows per tile).  Results are cached
+per (device name, shape or batch signature, mode) in memory and, when HS_AUTOTUNE_CACHE
+names a file, in that JSON file.  HS_AUTOTUNE_LOG names a file that receives every
+candidate's timing as one JSON line per tuning.
 """
 from __future__ import annotations
 
@@ -121,3 +123,69 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
 def clear():
     with _lock:
         _cache.clear()
+
+
+BATCH_CANDIDATES = ((3, 96), (4, 64), (4, 96), (5, 96), (5, 128), (6, 128))
+
+
+def _log(entry):
+    log = os.environ.get("HS_AUTOTUNE_LOG")
+    if log:
+        try:
+            with open(log, "a") as f:
+                f.write(json.dumps(entry) + "\n")
+        except OSError:
+            pass
+
+
+def best_batch_config(specs, fast_math: bool = True, candidates=BATCH_CANDIDATES,
+                      reps: int = 3) -> Tuple[int, int]:
+    """(sweeps_per_pass, rows_per_segment) fastest for the persistent batched launch of
+    `specs` = [(H, W, alpha, iters)] on the current device (timed as CUDA-graph replays
+    of the batch itself over seeded random planes)."""
+    import hashlib
+
+    import torch
+
+    from . import _lib as L
+    from .batched import BatchPlan
+
+    sig = hashlib.sha1(repr(sorted((int(H), int(W), float(a), int(n)) for H, W, a, n in specs))
+                       .encode()).hexdigest()[:16]
+    key = f"{torch.cuda.get_device_name()}|batch{len(specs)}:{sig}|{'fast' if fast_math else 'exact'}"
+    with _lock:
+        if not _cache:
+            _load_file()
+        if key in _cache:
+            return _cache[key]
+    g = torch.Generator(device="cuda")
+    g.manual_seed(0)
+    results = []
+    for T, rows in candidates:
+        plan = BatchPlan(specs, L.make_config(sweeps_per_pass=T, rows_per_segment=rows,
+                                              fast_math=fast_math))
+        for a, b in zip(plan.I0, plan.I1):
+            a.copy_(torch.rand(a.shape, device="cuda", generator=g))
+            b.copy_(torch.rand(b.shape, device="cuda", generator=g))
+        plan.capture()
+        plan.replay()
+        plan.check()
+        best = float("inf")
+        for _ in range(reps):
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            plan.replay()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        plan.check()
+        results.append((best, T, rows))
+        del plan
+    results.sort()
+    best = (results[0][1], results[0][2])
+    _log({"key": key, "ms": [[round(ms, 4), T, r] for ms, T, r in results]})
+    with _lock:
+        _cache[key] = best
+        _save_file()
+    return best

@@ -205,7 +205,7 @@ struct PairPlan {
 
 static int batch_seg_rows(int H, int T, int cfg_rows) {
     if (cfg_rows > 0) return std::max(std::min(cfg_rows, H), std::min(H, T));
-    return std::min(H, std::max(64, T));
+    return std::min(H, std::max(96, T));
 }
 
 static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *cfg,

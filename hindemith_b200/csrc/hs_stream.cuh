@@ -41,10 +41,16 @@ constexpr unsigned kFull = 0xffffffffu;
 
 template <int T>
 struct Geo {
-    static constexpr int halo = (T + 3) & ~3;                  // strips start 16-byte aligned
+    static constexpr int halo = (T + 1) & ~1;                  // even: lanes read float2
+    // Rows are copied in 16-byte chunks.  A strip starts at x0 = strip*i - halo, which is
+    // 16-byte aligned when halo % 4 == 0 ("wide": 16 chunks per plane row); otherwise the
+    // copy starts sh = 2 columns early and takes 17 chunks (68 floats) per plane row.
+    static constexpr bool wide = (halo % 4) == 0;
+    static constexpr int sh = wide ? 0 : 2;
+    static constexpr int rw = wide ? kWarpCols : kWarpCols + 4;  // floats per ring plane row
     static constexpr int strip = kWarpCols - 2 * halo;         // output columns per strip
     static constexpr int coef_slots = T + 1;                   // rows k-T .. k
-    static constexpr int raw_floats = kRawSlots * kRawPlanes * kWarpCols;
+    static constexpr int raw_floats = kRawSlots * kRawPlanes * rw;
     static constexpr int coef_floats = coef_slots * 2 * 32 * 4;  // [slot][column][lane] float4
     static constexpr int warp_floats = raw_floats + coef_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
@@ -160,21 +166,38 @@ struct Item {
     float alpha2;  // p.alpha2, or the square of the device-resident alpha
 };
 
-// A row of the strip is 5 planes x 64 floats = 80 chunks of 16 bytes; lane l copies
-// chunks l, l+32 and (lanes 0-15) l+64: planes u|v, Ix|Iy and It for lanes < 16 | >= 16.
+// Copy one row of the strip (5 planes) into ring slot `slot`, 16-byte chunks through L2
+// only (lanes copy chunks other lanes read, so each step brackets the copy and its wait
+// with warp barriers).
+//   wide: 80 chunks; lane l copies chunks l, l+32 and (lanes 0-15) l+64, i.e. planes u|v,
+//         Ix|Iy and It for lanes < 16 | >= 16;
+//   else: lanes 0-16 copy chunk `lane` of each of the 5 planes (68 floats per plane row).
+template <int T>
 __device__ __forceinline__ void issue_row(const Item &it, int slot, int row, const SweepParams &p) {
+    using G = Geo<T>;
     row = min(max(row, 0), p.H - 1);
     const size_t off = (size_t)row * p.ld + it.lcol;
-    const bool lo = it.lane < 16;
-    float *base = it.raw + slot * (kRawPlanes * kWarpCols) + 4 * (it.lane & 15);
-    cp_async16(base + (lo ? 0 : 1) * kWarpCols, (lo ? p.u_in : p.v_in) + off);
-    cp_async16(base + (lo ? 2 : 3) * kWarpCols, (lo ? p.Ix : p.Iy) + off);
-    if (lo) cp_async16(base + 4 * kWarpCols, p.It + off);
+    if constexpr (G::wide) {
+        const bool lo = it.lane < 16;
+        float *base = it.raw + slot * (kRawPlanes * G::rw) + 4 * (it.lane & 15);
+        cp_async16(base + (lo ? 0 : 1) * G::rw, (lo ? p.u_in : p.v_in) + off);
+        cp_async16(base + (lo ? 2 : 3) * G::rw, (lo ? p.Ix : p.Iy) + off);
+        if (lo) cp_async16(base + 4 * G::rw, p.It + off);
+    } else {
+        if (it.lane < G::rw / 4) {
+            float *base = it.raw + slot * (kRawPlanes * G::rw) + 4 * it.lane;
+            cp_async16(base + 0 * G::rw, p.u_in + off);
+            cp_async16(base + 1 * G::rw, p.v_in + off);
+            cp_async16(base + 2 * G::rw, p.Ix + off);
+            cp_async16(base + 3 * G::rw, p.Iy + off);
+            cp_async16(base + 4 * G::rw, p.It + off);
+        }
+    }
     cp_async_commit();
 }
 
 // One streaming step: row k arrives at stage 0, stage s emits sweep s+1 of row k-s-1.
-template <int T, bool FAST, bool XEDGE, bool EDGE>
+template <int T, bool FAST, bool XEDGE, bool EDGE, bool DUMP>
 __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it, Win<FAST> (&w)[T][2][2],
                                             int k, int rslot, int cslot) {
     // Prefetch row k + kPrefetch into the slot row k-1 used, then wait for row k (never
@@ -185,16 +208,17 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     // and the one before the prefetch keeps it from overwriting a slot another lane is
     // still reading.
     __syncwarp();
-    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + T), p);
+    issue_row<T>(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + T), p);
     cp_async_wait<kPrefetch>();
     __syncwarp();
 
     // stage 0: unpack row k; pack its coefficients with the denominator term
-    const float *raw = it.raw + rslot * (kRawPlanes * kWarpCols) + 2 * it.lane;
-    const float2 u2 = lds2(raw), v2 = lds2(raw + kWarpCols);
+    constexpr int RW = Geo<T>::rw;
+    const float *raw = it.raw + rslot * (kRawPlanes * RW) + Geo<T>::sh + 2 * it.lane;
+    const float2 u2 = lds2(raw), v2 = lds2(raw + RW);
     {
-        const float2 ix = lds2(raw + 2 * kWarpCols), iy = lds2(raw + 3 * kWarpCols);
-        const float2 t2 = lds2(raw + 4 * kWarpCols);
+        const float2 ix = lds2(raw + 2 * RW), iy = lds2(raw + 3 * RW);
+        const float2 t2 = lds2(raw + 4 * RW);
         float ax, ay;
         if constexpr (FAST) {
             ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
@@ -248,7 +272,7 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
                 cu[1][j] = __fsub_rn(vbar, __fmul_rn(C[j].y, t));
             }
         }
-        if (p.dump) {  // warp-uniform: write sweep s+1 of row k-s-1 (state dumps)
+        if constexpr (DUMP) {  // write sweep s+1 of row k-s-1 (state dumps)
             const int rr = k - s - 1;
             if (rr >= it.y_start && rr < it.y_end) {
                 const size_t off = (size_t)rr * p.ld + it.xa;
@@ -277,7 +301,7 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     }
 }
 
-template <int T, bool FAST, bool XEDGE>
+template <int T, bool FAST, bool XEDGE, bool DUMP>
 __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
@@ -290,7 +314,7 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
             for (int j = 0; j < 2; ++j) w[s][q][j] = Win<FAST>{};
 
 #pragma unroll
-    for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, p);
+    for (int i = 0; i < kPrefetch; ++i) issue_row<T>(it, i, k0 + i, p);
 
     // Steps in [klo, khi] have no stage at row 0 or past row H-2: no clamp logic.
     const int klo = max(k0, T);
@@ -302,11 +326,11 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
         cslot = (cslot + 1 == Geo<T>::coef_slots) ? 0 : cslot + 1;
     };
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) stream_step<T, FAST, XEDGE, true>(p, it, w, k, rslot, cslot);
+        for (; k < klo; advance()) stream_step<T, FAST, XEDGE, true, DUMP>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
-            stream_step<T, FAST, XEDGE, false>(p, it, w, k, rslot, cslot);
+            stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
-            stream_step<T, FAST, XEDGE, false>(p, it, w, k, rslot, cslot);
+            stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
         }
         // Here k <= H-1, so row H-1 reaches every stage in the tail loop below.  The
@@ -321,7 +345,7 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
                     for (int j = 0; j < 2; ++j) w[s][q][j].l1 = w[s][q][j].c1 = w[s][q][j].r1 = 0.f;
         }
     }
-    for (; k <= k_end; advance()) stream_step<T, FAST, XEDGE, true>(p, it, w, k, rslot, cslot);
+    for (; k <= k_end; advance()) stream_step<T, FAST, XEDGE, true, DUMP>(p, it, w, k, rslot, cslot);
     cp_async_wait<0>();
 }
 
@@ -356,10 +380,10 @@ __device__ __forceinline__ void init_item(Item &it, const SweepParams &p, int st
     it.lane = lane;
     it.xa = x0 + 2 * lane;
     const int xb = it.xa + 1;
-    // the lane's 16-byte chunk: x0 and ld are multiples of 4, so a chunk lies wholly inside
-    // or outside the row; outside ones copy any in-bounds chunk (their columns never
+    // the lane's 16-byte chunk: its start and ld are multiples of 4, so a chunk lies wholly
+    // inside or outside the row; outside ones copy any in-bounds chunk (their columns never
     // feed a stored pixel)
-    const int xc = x0 + 4 * (lane & 15);
+    const int xc = G::wide ? x0 + 4 * (lane & 15) : x0 - G::sh + 4 * lane;
     it.lcol = (xc >= 0 && xc + 4 <= p.ld) ? xc : 0;
     it.lc2 = (it.xa >= 0 && it.xa < p.W) ? it.xa : 0;  // xa is even and ld % 4 == 0
     it.a_first = (it.xa == 0);
@@ -374,11 +398,13 @@ __device__ __forceinline__ void init_item(Item &it, const SweepParams &p, int st
 }
 
 // Run one work item; only strips reaching an image side need the horizontal clamps.
-template <int T, bool FAST>
+// DUMP (the training recompute) also writes every stage's sweep to p.dump_u/v; it is a
+// template parameter so the plain kernels carry no per-stage branch.
+template <int T, bool FAST, bool DUMP = false>
 __device__ __forceinline__ void run_item(const SweepParams &p, const Item &it) {
     const int x0 = it.xa - 2 * it.lane;
-    if (x0 <= 0 || x0 + kWarpCols >= p.W) stream_item<T, FAST, true>(p, it);
-    else stream_item<T, FAST, false>(p, it);
+    if (x0 <= 0 || x0 + kWarpCols >= p.W) stream_item<T, FAST, true, DUMP>(p, it);
+    else stream_item<T, FAST, false, DUMP>(p, it);
 }
 
 }  // namespace hs

@@ -30,8 +30,9 @@ namespace hs {
 
 constexpr int kMaxTrainPairs = 32;
 constexpr int kMaxTB = 5;
+constexpr int kAdjMaxDepth = 4;     // deepest adjoint pass the backward plans
 constexpr int kAdjItemsPerSm = 12;  // adjoint work items (warps) per SM and launch
-constexpr int kMinStripCols = 48;   // narrowest strip: 64 columns less a halo of 8 each side
+constexpr int kMinStripCols = 52;   // narrowest adjoint strip (depth <= 5): 64 less 6 each side
 
 // ------------------------------------------------------------------ table-driven pass
 
@@ -67,7 +68,8 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
     const int local = item - tab.item_prefix[pi];
     Item it;
     init_item<T>(it, p, local % p.nstrips, local / p.nstrips, lane, wbase);
-    run_item<T, FAST>(p, it);
+    if (p.dump) run_item<T, FAST, true>(p, it);
+    else run_item<T, FAST, false>(p, it);
 }
 
 template <int T, bool FAST>
@@ -126,7 +128,7 @@ struct AdjTable {
 template <int TB>
 struct AdjGeo {
     static constexpr int coef_slots = TB + 1;
-    static constexpr int raw_floats = kRawSlots * kRawPlanes * kWarpCols;
+    static constexpr int raw_floats = Geo<TB>::raw_floats;
     static constexpr int ring_floats = coef_slots * 2 * 2 * 32 * 4;  // [slot][coef|acc][col][lane] float4
     static constexpr int warp_floats = raw_floats + ring_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
@@ -168,17 +170,18 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
                                          float we, float wc, int k, int rslot, int cslot,
                                          float2 (&xs)[TB][2], float &a2s) {
     __syncwarp();
-    issue_row(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
+    issue_row<TB>(it, (rslot + kPrefetch) & (kRawSlots - 1), min(k + kPrefetch, it.y_end - 1 + TB), lp);
     cp_async_wait<kPrefetch>();
     __syncwarp();
 
     // stage 0: lambda row k arrives; coefficients, zeroed accumulators, then M
-    const float *raw = it.raw + rslot * (kRawPlanes * kWarpCols) + 2 * it.lane;
-    const float2 l2u = lds2(raw), l2v = lds2(raw + kWarpCols);
+    constexpr int RW = Geo<TB>::rw;
+    const float *raw = it.raw + rslot * (kRawPlanes * RW) + Geo<TB>::sh + 2 * it.lane;
+    const float2 l2u = lds2(raw), l2v = lds2(raw + RW);
     float cu[2][2];
     {
-        const float2 ix = lds2(raw + 2 * kWarpCols), iy = lds2(raw + 3 * kWarpCols);
-        const float2 t2 = lds2(raw + 4 * kWarpCols);
+        const float2 ix = lds2(raw + 2 * RW), iy = lds2(raw + 3 * RW);
+        const float2 t2 = lds2(raw + 4 * RW);
         const float ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
         const float ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
         const float4 C[2] = {make_float4(ix.x, iy.x, t2.x, ax), make_float4(ix.y, iy.y, t2.y, ay)};
@@ -287,7 +290,7 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
 #pragma unroll
             for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
 #pragma unroll
-    for (int i = 0; i < kPrefetch; ++i) issue_row(it, i, k0 + i, lp);
+    for (int i = 0; i < kPrefetch; ++i) issue_row<TB>(it, i, k0 + i, lp);
     float2 xs[TB][2];
     float a2s = 0.f;
     adj_prefetch<TB>(P, it, k0, xs);
@@ -639,7 +642,8 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
     }
     HS_CUDA_CHECK(cudaMemsetAsync(ws + L.partials_off, 0, (size_t)n * L.nslots * sizeof(double), s));
     int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
-    const int TB = std::min(kMaxTB, std::max(1, rc.T));
+    // adjoint depth: at most 4 (a 5-deep adjoint pass is register-bound and slower)
+    const int TB = std::min(kAdjMaxDepth, std::max(1, rc.T));
     for (int b = L.nb - 1; b >= 0; --b) {
         const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
         // 1. states x_{k_lo+1} .. x_{k_lo+nsw-1} into states[0..nsw-2]
