@@ -49,9 +49,13 @@ def parse_args():
     ap.add_argument("--batch-pairs", type=int, default=64,
                     help="pairs of the mixed batch (a prefix of the 64-pair list)")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batch-sweeps-per-pass", type=int, default=0,
+                    help="batched leg: sweeps per pass (0 = autotuned with the rows per tile)")
+    ap.add_argument("--batch-rows", type=int, default=0, help="batched leg: rows per tile")
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--train-sweeps-per-pass", type=int, default=5)
     ap.add_argument("--no-pyramid", action="store_true")
+    ap.add_argument("--no-cg", action="store_true")
     ap.add_argument("--pyramid-pairs", type=int, default=8)
     return ap.parse_args()
 
@@ -222,7 +226,10 @@ def measure_batched(args, rank, flush, peak):
     for sp in specs:
         sp.seed += 100 * rank
     shape = [(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs]
-    T, rows = best_batch_config(shape, fast_math=not args.exact)
+    if args.batch_sweeps_per_pass > 0:
+        T, rows = args.batch_sweeps_per_pass, args.batch_rows
+    else:
+        T, rows = best_batch_config(shape, fast_math=not args.exact)
     cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=rows, fast_math=not args.exact)
     plan = BatchPlan([(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs], cfg)
     for i, sp in enumerate(specs):
@@ -248,7 +255,7 @@ def measure_batched(args, rank, flush, peak):
     return {
         "workload": f"hs_batched_{len(specs)}pairs_mixed", "pairs": len(specs),
         "mpix": round(sum(sp.H * sp.W for sp in specs) / 1e6, 3), "pix_iters": px_it,
-        "sweeps_per_pass": T, "rows_per_tile": rows, "autotuned": True,
+        "sweeps_per_pass": T, "rows_per_tile": rows, "autotuned": args.batch_sweeps_per_pass == 0,
         "launch": "one persistent kernel per batch, CUDA graph replay",
         "value": px_it * args.steps / t_b / 1e6, "unit": UNIT,
         "ms_per_step": t_b / args.steps * 1e3,
@@ -374,6 +381,49 @@ def measure_pyramid(args, rank, flush):
             "loss": loss, "peak_device_bytes": int(max(eager_peak, graph_peak)),
             "peak_device_bytes_eager": int(eager_peak), "peak_device_bytes_graph": int(graph_peak),
             "input_bytes": int(base)}
+
+
+def measure_cg(args, rank, flush, peak):
+    """Horn-Schunck as a linear system at 2048x2048: 9 Krylov powers of the HS operator
+    (hs_matrix_powers, 4 powers per pass) and one block-Jacobi preconditioner application,
+    as HBM GB/s against the measured peak."""
+    import torch
+
+    from hindemith_b200 import _lib as L
+    from hindemith_b200 import cg
+    from hindemith_b200 import device as D
+
+    H = W = 2048
+    g = torch.Generator(device="cuda")
+    g.manual_seed(5 + rank)
+    planes = D.empty_planes(7, H, W)
+    for p in planes:
+        p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
+    Ix, Iy, r0, r1, d0, d1, od = planes
+    steps, depth = 9, 4
+    cfg = L.make_config(sweeps_per_pass=depth)
+    stream = torch.cuda.current_stream()
+    k = max(1, args.steps)
+
+    def powers():
+        cg.hs_matrix_powers(0.5, Ix, Iy, r0, r1, steps, cfg)
+
+    def precond():
+        cg.apply_hs_preconditioner(0.25, d0, d1, od, r0, r1)
+
+    t_mp = timed_events(powers, k, 3, flush, stream, "timed_matrix_powers")
+    t_pc = timed_events(precond, k, 3, flush, stream, "timed_preconditioner")
+    passes = (steps - 1 + depth - 1) // depth
+    mp_bytes = H * W * (16 * passes + 8 * (steps - 1) + 16)  # + the copy of V[0]
+    pc_bytes = H * W * 28
+    mp_gbs = mp_bytes * k / t_mp / 1e9
+    pc_gbs = pc_bytes * k / t_pc / 1e9
+    return {"workload": "hs_matrix_powers_2048x2048_9steps + hs_apply_hs_preconditioner_2048x2048",
+            "matrix_powers": {"ms": t_mp / k * 1e3, "powers_per_pass": depth,
+                              "bytes_per_call": mp_bytes, "achieved_gbs": mp_gbs,
+                              "frac": mp_gbs / peak},
+            "preconditioner": {"ms": t_pc / k * 1e3, "bytes_per_call": pc_bytes,
+                               "achieved_gbs": pc_gbs, "frac": pc_gbs / peak}}
 
 
 # ------------------------------------------------------------------ GPU arm
@@ -532,6 +582,8 @@ def main():
         line["batched"] = measure_batched(args, rank, flush, peak)
     if world == 1 and not args.no_train and not args.shape:
         line["fwd_bwd"] = measure_train(args, rank, flush)
+    if world == 1 and not args.no_cg and not args.shape:
+        line["cg"] = measure_cg(args, rank, flush, peak)
     if world == 1 and not args.no_pyramid and not args.shape:
         line["pyramid"] = measure_pyramid(args, rank, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -119,6 +119,8 @@ SIGNATURES = {
     "hs_train_workspace_bytes": (_sz, [_tpp, _i, _i, _i]),
     "hs_forward_train_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
+    "hs_matrix_powers": (_i, [_f, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _sz, _cfgp, _vp]),
+    "hs_apply_hs_preconditioner": (_i, [_f, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
     "hs_epe_workspace_bytes": (_sz, [_i]),
     "hs_epe_loss_batched": (_i, [_epp, _i, _f, _vp, _vp, _sz, _vp]),
     "hs_epe_loss_backward_batched": (_i, [_epp, _i, _f, _vp, _vp]),

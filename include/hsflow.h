@@ -250,6 +250,31 @@ HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *
                                  const float *ddst, int H, int W, int ld, float *dsrc, float *du,
                                  float *dv, void *stream);
 
+/* ---- Horn-Schunck as a linear system (CG family) ------------------------------ */
+
+/* Krylov powers of the HS normal-equations operator, HSMatrixPowers.cpp:72-106 (setup
+ * :129-226): V[0] = (r0, r1) and V[s] = M V[s-1] for s = 1 .. steps-1, where
+ *   M(u, v) = (Ix g, Iy g) + lam (deg u - sum of the 4-neighbours of u, same for v),
+ *   g = Ix u + Iy v, neighbours outside the image absent,
+ * in the template's operation order (bit-identical to its FP32 semantics).  V0, V1 hold
+ * `steps` planes each, power s at V + s * power_stride floats (power_stride >= H*ld, a
+ * multiple of 4).  cfg->sweeps_per_pass (1..4, 0 = 4) powers are computed per pass over
+ * HBM from one shared-memory tile. */
+HS_API hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const float *r0,
+                                  const float *r1, int H, int W, int ld, int steps, float *V0,
+                                  float *V1, size_t power_stride, const hs_config *cfg,
+                                  void *stream);
+
+/* The 2x2 block-Jacobi preconditioner of the HS system, ApplyHSPreconditioner.cpp:46-97:
+ *   a = diag0 + n s2, d = diag1 + n s2 (n = neighbours present), b = c = offdiag,
+ *   det = a d - b c; |det| > 1e-15: y0 = (x0 d - b x1)/det, y1 = (-c x0 + a x1)/det;
+ *   else y = x.
+ * s2 is the stencil's third weight (the template's getData("2")). */
+HS_API hs_status hs_apply_hs_preconditioner(float s2, const float *diag0, const float *diag1,
+                                            const float *offdiag, const float *x0,
+                                            const float *x1, int H, int W, int ld, float *y0,
+                                            float *y1, void *stream);
+
 /* ---- loss ------------------------------------------------------------------- */
 
 /* One flow field and its target for the mean end-point-error loss; du, dv receive the

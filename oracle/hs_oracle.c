@@ -332,3 +332,69 @@ HSO_API void hso_warp_f32(const float *src, const float *ox, const float *oy, in
         }
     }
 }
+
+/* ------------------------------------------------------------------ CG family */
+
+/* HSMatrixPowers.cpp:72-106 (element template) and :129-226 (setup): V[0] = r; for
+ * s = 1 .. steps-1, V[s] = M V[s-1] with the Horn-Schunck normal-equations operator
+ *   ures = Ix*(Ix*u + Iy*v);  vres = Iy*(Ix*u + Iy*v)
+ *   for each neighbour n present, in the order left (x > 0), right (x < W-1),
+ *   up (y > 0), down (y < H-1):  res += -lam*n;  res += lam*mid
+ * V is (steps, H, W), step slowest.  One rounding per operation, in template order. */
+HSO_API void hso_hs_matrix_powers_f32(float lam, const float *Ix, const float *Iy, const float *r0,
+                                      const float *r1, int H, int W, int steps, float *V0,
+                                      float *V1) {
+    const size_t n = (size_t)H * W;
+    memcpy(V0, r0, n * sizeof(float));
+    memcpy(V1, r1, n * sizeof(float));
+    const float nl = -lam;
+    for (int s = 1; s < steps; ++s) {
+        const float *u = V0 + (size_t)(s - 1) * n, *v = V1 + (size_t)(s - 1) * n;
+        float *uo = V0 + (size_t)s * n, *vo = V1 + (size_t)s * n;
+#pragma omp parallel for schedule(static)
+        for (int y = 0; y < H; ++y) {
+            for (int x = 0; x < W; ++x) {
+                const size_t i = (size_t)y * W + x;
+                const float um = u[i], vm = v[i], ix = Ix[i], iy = Iy[i];
+                const float g = ix * um + iy * vm;
+                float ur = ix * g, vr = iy * g;
+                if (x > 0) { ur += nl * u[i - 1]; vr += nl * v[i - 1]; ur += lam * um; vr += lam * vm; }
+                if (x < W - 1) { ur += nl * u[i + 1]; vr += nl * v[i + 1]; ur += lam * um; vr += lam * vm; }
+                if (y > 0) { ur += nl * u[i - W]; vr += nl * v[i - W]; ur += lam * um; vr += lam * vm; }
+                if (y < H - 1) { ur += nl * u[i + W]; vr += nl * v[i + W]; ur += lam * um; vr += lam * vm; }
+                uo[i] = ur;
+                vo[i] = vr;
+            }
+        }
+    }
+}
+
+/* ApplyHSPreconditioner.cpp:46-97: the 2x2 block-Jacobi preconditioner of the HS system.
+ *   a = diag0, d = diag1, each plus s for every neighbour present (x < W-1, y < H-1, x > 0,
+ *   y > 0; s = the stencil's data[2]);  det = a*d - b*c (b = c = offdiag);
+ *   |det| > 1e-15:  y0 = (x0*d - b*x1)/det,  y1 = (-c*x0 + a*x1)/det;  else y = x.
+ * (hlib.applyHSPreconditioner, hlib.py:18-47, is the NumPy form; it tests |det| > 1e-4.) */
+HSO_API void hso_apply_hs_precond_f32(float s2, const float *diag0, const float *diag1,
+                                      const float *offdiag, const float *x0, const float *x1,
+                                      int H, int W, float *y0, float *y1) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const size_t i = (size_t)y * W + x;
+            float a = diag0[i], d = diag1[i];
+            if (x < W - 1) { a += s2; d += s2; }
+            if (y < H - 1) { a += s2; d += s2; }
+            if (x > 0) { a += s2; d += s2; }
+            if (y > 0) { a += s2; d += s2; }
+            const float b = offdiag[i], c = offdiag[i], e = x0[i], f = x1[i];
+            const float det = a * d - b * c;
+            if (fabsf(det) > 1e-15f) {
+                y0[i] = (e * d - b * f) / det;
+                y1[i] = (-c * e + a * f) / det;
+            } else {
+                y0[i] = e;
+                y1[i] = f;
+            }
+        }
+    }
+}

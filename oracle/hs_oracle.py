@@ -177,6 +177,10 @@ def lib():
         L.hso_hs_forward_f32.argtypes = [f32p, f32p, c_int, c_int, c_float, c_int, f32p, f32p]
         L.hso_hs_forward_f64.argtypes = [f64p, f64p, c_int, c_int, c_double, c_int, f64p, f64p]
         L.hso_warp_f32.argtypes = [f32p, f32p, f32p, c_int, c_int, f32p]
+        L.hso_hs_matrix_powers_f32.argtypes = [c_float, f32p, f32p, f32p, f32p, c_int, c_int,
+                                               c_int, f32p, f32p]
+        L.hso_apply_hs_precond_f32.argtypes = [c_float, f32p, f32p, f32p, f32p, f32p, c_int,
+                                               c_int, f32p, f32p]
         for name in ("hso_hs_sweeps_f32", "hso_hs_sweeps_f64", "hso_hs_forward_f32",
                      "hso_hs_forward_f64"):
             getattr(L, name).restype = c_int
@@ -259,6 +263,45 @@ def c_warp(src, ox, oy):
     out = np.empty_like(src)
     lib().hso_warp_f32(src, ox, oy, H, W, out)
     return out
+
+
+def c_hs_matrix_powers(lam, Ix, Iy, r0, r1, steps):
+    """HSMatrixPowers.cpp:72-106 in FP32, template operation order -> V0, V1 (steps, H, W)."""
+    Ix, Iy, r0, r1 = _c32(Ix), _c32(Iy), _c32(r0), _c32(r1)
+    H, W = Ix.shape
+    V0 = np.empty((steps, H, W), np.float32)
+    V1 = np.empty((steps, H, W), np.float32)
+    lib().hso_hs_matrix_powers_f32(float(np.float32(lam)), Ix, Iy, r0, r1, H, W, int(steps), V0, V1)
+    return V0, V1
+
+
+def c_apply_hs_precond(s2, diag0, diag1, offdiag, x0, x1):
+    """ApplyHSPreconditioner.cpp:46-97 in FP32 -> y0, y1."""
+    diag0, diag1, offdiag, x0, x1 = (_c32(a) for a in (diag0, diag1, offdiag, x0, x1))
+    H, W = x0.shape
+    y0, y1 = np.empty_like(x0), np.empty_like(x0)
+    lib().hso_apply_hs_precond_f32(float(np.float32(s2)), diag0, diag1, offdiag, x0, x1, H, W, y0, y1)
+    return y0, y1
+
+
+def hs_normal_matrix(lam, Ix, Iy):
+    import scipy.sparse as sp
+
+    Ix = np.asarray(Ix, np.float64)
+    Iy = np.asarray(Iy, np.float64)
+    H, W = Ix.shape
+
+    def lap1(n):
+        if n == 1:
+            return sp.csr_matrix((1, 1))
+        main = np.full(n, 2.0)
+        main[0] = main[-1] = 1.0
+        return sp.diags([main, -np.ones(n - 1), -np.ones(n - 1)], [0, -1, 1])
+
+    L = sp.kron(sp.identity(H), lap1(W)) + sp.kron(lap1(H), sp.identity(W))
+    ix, iy = Ix.ravel(), Iy.ravel()
+    return sp.bmat([[sp.diags(ix * ix) + lam * L, sp.diags(ix * iy)],
+                    [sp.diags(ix * iy), sp.diags(iy * iy) + lam * L]]).tocsr()
 
 
 # ---------------------------------------------------------------- adjoint (FP64)

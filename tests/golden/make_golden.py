@@ -24,6 +24,7 @@ Fixtures (tests/golden/*.npz):
   stencil_*.npz  : x, weights, offx, offy, out      (Stencil * Array2D)
   hs_*.npz       : I0, I1, alpha2, sweeps, Ix, Iy, It, u, v   (hs_programs.hs_jacobi)
   warp_*.npz     : src, ox, oy, out                 (warp_img2d, integer offsets)
+  precond_*.npz  : s2, d0_i, d1_i, od_i, x0_i, x1_i, y0_i, y1_i   (applyHSPreconditioner)
 """
 from __future__ import annotations
 
@@ -146,6 +147,27 @@ def main(ref_root: str):
         np.savez_compressed(os.path.join(out_dir, f"warp_{fname}.npz"), src=src,
                             ox=ox.astype(np.float32), oy=oy.astype(np.float32),
                             out=np.asarray(out, dtype=np.float32))
+    # applyHSPreconditioner (hlib.py:18-47): the block-Jacobi step of the HS system.  Its
+    # determinant guard (|det| > 1e-4) differs from the device template's (> 1e-15); the
+    # random case keeps every |det| above 1e-4 so that both guards agree, and the zero
+    # case has det = 0 exactly (both copy x through).
+    prng = np.random.Generator(np.random.PCG64(11))
+    for cname, scale in (("rand", 1.0), ("zero", 0.0)):
+        arrs = {}
+        for i, (H, W) in enumerate([(1, 1), (1, 5), (6, 1), (13, 17)]):
+            d0 = (prng.uniform(0.1, 1.0, (H, W)) * scale).astype(np.float32)
+            d1 = (prng.uniform(0.1, 1.0, (H, W)) * scale).astype(np.float32)
+            od = (prng.uniform(-0.05, 0.05, (H, W)) * scale).astype(np.float32)
+            x0 = prng.standard_normal((H, W)).astype(np.float32)
+            x1 = prng.standard_normal((H, W)).astype(np.float32)
+            sdata = np.float32([0.0, 0.0, 0.25 * scale, 0.0])
+            D = hl.Stencil(sdata, np.int64([0, 1, 0, 1]), np.int64([0, 0, 1, 1]))
+            y0, y1 = hl.applyHSPreconditioner(D, d0, d1, od, x0, x1)
+            arrs.update({f"d0_{i}": d0, f"d1_{i}": d1, f"od_{i}": od, f"x0_{i}": x0,
+                         f"x1_{i}": x1, f"y0_{i}": np.asarray(y0, np.float32),
+                         f"y1_{i}": np.asarray(y1, np.float32)})
+        np.savez_compressed(os.path.join(out_dir, f"precond_{cname}.npz"),
+                            s2=np.float32(0.25 * scale), n=np.int32(4), **arrs)
     print("wrote fixtures to", out_dir)
 
 

@@ -165,3 +165,17 @@ def test_epe_argument_checks_before_launch():
     d[1].ld = 4
     # the backward needs gradient planes
     assert lib.hs_epe_loss_backward_batched(d, 2, 0.0, P, None) == L.HS_ERR_INVALID_ARG
+
+
+def test_cg_family_argument_checks():
+    lib = L.lib()
+    P = fake_ptr()
+    cfg = L.make_config()
+    assert lib.hs_matrix_powers(1.0, P, P, P, P, 8, 8, 8, 0, P, P, 64, ctypes.byref(cfg), None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_matrix_powers(1.0, P, P, P, P, 8, 8, 8, 3, P, P, 32, ctypes.byref(cfg), None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_matrix_powers(1.0, P, P, None, P, 8, 8, 8, 3, P, P, 64, ctypes.byref(cfg), None) == L.HS_ERR_INVALID_ARG
+    deep = L.make_config(sweeps_per_pass=5)
+    assert lib.hs_matrix_powers(1.0, P, P, P, P, 8, 8, 8, 3, P, P, 64, ctypes.byref(deep), None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, P, P, 8, 6, 6, P, P, None) == L.HS_ERR_ALIGNMENT
+    assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, P, P, 0, 8, 8, P, P, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, fake_ptr(8), P, 8, 8, 8, P, P, None) == L.HS_ERR_ALIGNMENT

@@ -188,3 +188,44 @@ def test_torch_pyramid_reference_matches_oracle():
         ox, oy = rng.uniform(-3, 3, (H, W)), rng.uniform(-3, 3, (H, W))
         np.testing.assert_allclose(warp_torch(torch.tensor(x), torch.tensor(ox), torch.tensor(oy)).numpy(),
                                    O.warp_f64(x, ox, oy), rtol=0, atol=1e-14)
+
+
+def test_hs_average_is_self_adjoint():
+    """A^T = A for the clamp-to-edge 3x3 HS average (what lets the adjoint sweep stream
+    with the forward's skeleton): the transposed stencil equals the stencil itself."""
+    rng = np.random.default_rng(11)
+    w = O.AVG_W.astype(np.float64)
+    for (H, W) in ((1, 1), (1, 5), (4, 1), (2, 2), (3, 7), (16, 13)):
+        y = rng.standard_normal((H, W))
+        np.testing.assert_allclose(O.c_stencil2d_transpose(w, O.AVG_OFFX, O.AVG_OFFY, y),
+                                   O.c_stencil2d(w, O.AVG_OFFX, O.AVG_OFFY, y, np.float64),
+                                   rtol=0, atol=1e-15)
+
+
+def test_precond_oracle_matches_reference_golden():
+    """ApplyHSPreconditioner restatement vs hlib.applyHSPreconditioner (golden fixtures):
+    bit-identical where both determinant guards agree (all of the fixtures)."""
+    for name in ("precond_rand", "precond_zero"):
+        g = golden(name + ".npz")
+        for i in range(int(g["n"])):
+            y0, y1 = O.c_apply_hs_precond(g["s2"], g[f"d0_{i}"], g[f"d1_{i}"], g[f"od_{i}"],
+                                          g[f"x0_{i}"], g[f"x1_{i}"])
+            assert_bitexact(y0, g[f"y0_{i}"])
+            assert_bitexact(y1, g[f"y1_{i}"])
+
+
+def test_matrix_powers_oracle_matches_sparse_operator():
+    """HSMatrixPowers restatement vs the HS normal-equations operator assembled
+    independently as a sparse FP64 matrix (FP32 vs FP64: 1e-5 relative)."""
+    rng = np.random.default_rng(23)
+    for (H, W) in ((1, 1), (1, 6), (5, 1), (9, 13)):
+        Ix, Iy, r0, r1 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(4))
+        lam = np.float32(0.8)
+        V0, V1 = O.c_hs_matrix_powers(lam, Ix, Iy, r0, r1, 5)
+        M = O.hs_normal_matrix(np.float64(lam), Ix, Iy)
+        x = np.concatenate([r0.ravel(), r1.ravel()]).astype(np.float64)
+        for s in range(5):
+            ref = x / max(np.abs(x).max(), 1e-30)
+            got = np.concatenate([V0[s].ravel(), V1[s].ravel()]) / max(np.abs(x).max(), 1e-30)
+            assert np.abs(got - ref).max() < 1e-5
+            x = M @ x
