@@ -61,6 +61,16 @@ class hs_pair_desc(ctypes.Structure):
 HS_MAX_BATCH = 128
 
 
+HS_FUSED_MAX_IN, HS_FUSED_MAX_OUT, HS_FUSED_MAX_SCALARS, HS_FUSED_MAX_SUMS = 16, 8, 64, 8
+
+
+class hs_fused_args(ctypes.Structure):
+    _fields_ = [("in_", ctypes.c_void_p * HS_FUSED_MAX_IN), ("out", ctypes.c_void_p * HS_FUSED_MAX_OUT),
+                ("s", ctypes.c_float * HS_FUSED_MAX_SCALARS), ("H", ctypes.c_int),
+                ("W", ctypes.c_int), ("ld", ctypes.c_int), ("nsums", ctypes.c_int),
+                ("sums", ctypes.c_void_p), ("reserved", ctypes.c_int * 4)]
+
+
 class hs_epe_pair(ctypes.Structure):
     _fields_ = [("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("ut", ctypes.c_void_p),
                 ("vt", ctypes.c_void_p), ("du", ctypes.c_void_p), ("dv", ctypes.c_void_p),
@@ -121,6 +131,8 @@ SIGNATURES = {
     "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_matrix_powers": (_i, [_f, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _sz, _cfgp, _vp]),
     "hs_apply_hs_preconditioner": (_i, [_f, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
+    "hs_fused_workspace_bytes": (_sz, [_i, _i, _i]),
+    "hs_fused_launch": (_i, [ctypes.c_char_p, _i, ctypes.POINTER(hs_fused_args), _vp, _sz, _vp]),
     "hs_epe_workspace_bytes": (_sz, [_i]),
     "hs_epe_loss_batched": (_i, [_epp, _i, _f, _vp, _vp, _sz, _vp]),
     "hs_epe_loss_backward_batched": (_i, [_epp, _i, _f, _vp, _vp]),

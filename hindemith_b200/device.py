@@ -235,3 +235,15 @@ def hs_forward(I0, I1, alpha: float, iters: int, config: Optional[L.hs_config] =
                                ptr(u), ptr(v), ptr(ws), ws.numel(), ctypes.byref(cfg),
                                stream_handle(stream)), "hs_forward")
     return u, v
+
+
+def warp(src, u, v, stream=None) -> torch.Tensor:
+    """WarpImg2D: src backward-warped by (u, v) (Operations/OpticalFlow/WarpImg2D.cpp:33-75)."""
+    src, u, v = _same_layout(src, u, v)
+    if u.shape != src.shape or v.shape != src.shape:
+        raise ValueError("warp_img2d needs src, u and v of one shape")
+    out = _like(src)
+    H, W = src.shape
+    L.check(L.lib().hs_warp(ptr(src), ptr(u), ptr(v), H, W, ld_of(src), ptr(out),
+                            stream_handle(stream)), "hs_warp")
+    return out

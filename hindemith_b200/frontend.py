@@ -36,12 +36,18 @@ import numpy as np
 from . import _lib as L
 from .hlib import Stencil, hs_average_weights
 
-ARRAY2D, STENCIL, SCALAR = "Array2D", "Stencil", "Scalar"
+ARRAY2D, STENCIL, SCALAR, ARRAY3D = "Array2D", "Stencil", "Scalar", "Array3D"
 _OPS = {ast.Add: "Add", ast.Sub: "Sub", ast.Mult: "Mult", ast.Div: "Div"}
 
 
 class HMCompileError(TypeError):
     """The function uses a construct the Hindemith surface does not support."""
+
+
+def _call_name(node) -> str:
+    if not isinstance(node.func, ast.Name):
+        raise HMCompileError("only calls of plain function names are supported")
+    return node.func.id
 
 
 # ------------------------------------------------------------------ IR
@@ -146,14 +152,78 @@ class _Compiler:
                 raise HMCompileError(f"no operation matches {ka} {op} {kb}")
             self.kinds[name] = kind
             return name, kind
+        if isinstance(node, ast.Call):
+            names, kinds = self.call(node, out)
+            if len(names) != 1:
+                raise HMCompileError(f"{_call_name(node)}() returns {len(names)} values: assign them "
+                                     "to a tuple")
+            return names[0], kinds[0]
         if isinstance(node, ast.Tuple):
             raise HMCompileError("tuples are only supported in assignments and returns")
         raise HMCompileError(f"unsupported expression {type(node).__name__}")
+
+    def call(self, node, out: List[Stmt]) -> Tuple[List[str], List[str]]:
+        """The reference's call templates (Templates.py): sqrt (:485-534), sum2d (:468-483),
+        red / black (:536-568), warp_img2d (:258-275), applyHSPreconditioner (:412-443) and
+        hs_matrix_powers (:277-300).  Returns the result names and kinds."""
+        fname = _call_name(node)
+        if node.keywords:
+            raise HMCompileError(f"{fname}() takes positional arguments only")
+        args = [self.expr(a, out) for a in node.args]
+        kinds = [k for _, k in args]
+        names = [n for n, _ in args]
+
+        def want(sig):
+            if kinds != list(sig):
+                raise HMCompileError(f"{fname}({', '.join(kinds)}): expected ({', '.join(sig)})")
+
+        def one(kind, stmt_kind, **kw):
+            name = self.fresh()
+            out.append(Stmt(stmt_kind, name, tuple(names), **kw))
+            self.kinds[name] = kind
+            return [name], [kind]
+
+        if fname == "sqrt":
+            if kinds == [ARRAY2D]:
+                return one(ARRAY2D, "Array2DSqrt")
+            if kinds == [SCALAR]:
+                return one(SCALAR, "ScalarSqrt")
+            want([ARRAY2D])
+        if fname in ("sum2d", "sum"):
+            want([ARRAY2D])
+            return one(SCALAR, "Array2DSum")
+        if fname in ("red", "black"):
+            want([ARRAY2D])
+            return one(ARRAY2D, "RedArray2D" if fname == "red" else "BlackArray2D")
+        if fname == "warp_img2d":
+            want([ARRAY2D] * 3)
+            return one(ARRAY2D, "WarpImg2D")
+        if fname in ("applyHSPreconditioner", "hs_matrix_powers"):
+            if fname == "applyHSPreconditioner":
+                want([STENCIL] + [ARRAY2D] * 5)
+                kind, res = "ApplyHSPreconditioner", ARRAY2D
+            else:
+                want([SCALAR, ARRAY2D, ARRAY2D, ARRAY2D, ARRAY2D])
+                kind, res = "HSMatrixPowers", ARRAY3D
+            dsts = (self.fresh(), self.fresh())
+            out.append(Stmt(kind, None, tuple(names), info={"dsts": dsts}))
+            for d in dsts:
+                self.kinds[d] = res
+            return list(dsts), [res, res]
+        raise HMCompileError(f"unsupported call {fname}()")
 
     def assign(self, targets, value, out: List[Stmt]) -> None:
         if len(targets) != 1:
             raise HMCompileError("chained assignment is not supported")
         tgt = targets[0]
+        if isinstance(tgt, ast.Tuple) and isinstance(value, ast.Call):
+            names, kinds = self.call(value, out)
+            if len(names) != len(tgt.elts):
+                raise HMCompileError(f"{_call_name(value)}() returns {len(names)} values, "
+                                     f"{len(tgt.elts)} targets given")
+            for t, name, kind in zip(tgt.elts, names, kinds):
+                self._bind(t, name, kind, out)
+            return
         if isinstance(tgt, ast.Tuple):
             if not isinstance(value, ast.Tuple) or len(value.elts) != len(tgt.elts):
                 raise HMCompileError("tuple assignment needs a tuple of the same length")
@@ -180,7 +250,8 @@ class _Compiler:
         prev = self.kinds.get(tgt.id)
         if prev is not None and prev != kind:
             raise HMCompileError(f"'{tgt.id}' changes kind from {prev} to {kind}")
-        out.append(Stmt("Array2DCopy" if kind == ARRAY2D else "ScalarCopy", tgt.id, (name,)))
+        copy = {ARRAY2D: "Array2DCopy", SCALAR: "ScalarCopy", ARRAY3D: "Array3DCopy"}[kind]
+        out.append(Stmt(copy, tgt.id, (name,)))
         self.kinds[tgt.id] = kind
 
     def block(self, stmts, out: List[Stmt]) -> None:
@@ -427,9 +498,13 @@ class Executor:
     """Runs a Program on the current CUDA device (execute.cpp's role)."""
 
     def __init__(self, prog: Program, defines: Dict[str, Any]):
+        from .fusion import fuse_program
+
         self.prog = prog
         self.defines = dict(defines)
-        self.stats = {"hs_sweeps_calls": 0, "unfused_loops": 0}
+        self.stats = {"hs_sweeps_calls": 0, "unfused_loops": 0, "fused_launches": 0}
+        if self.defines.get("hs_fuse", True):
+            fuse_program(self.prog)
 
     def config(self) -> L.hs_config:
         d = self.defines
@@ -497,8 +572,39 @@ class Executor:
             env[s.dst] = -np.float32(env[s.args[0]])
         elif k == "Const":
             env[s.dst] = s.args[0]
-        elif k in ("Array2DCopy", "ScalarCopy"):
+        elif k in ("Array2DCopy", "ScalarCopy", "Array3DCopy"):
             env[s.dst] = env[s.args[0]]  # values are never updated in place: rebinding is a copy
+        elif k == "Fused":
+            from .fusion import run_group, split_group
+
+            fast = bool(self.defines.get("hs_fast_math", False))
+            if not run_group(s, env, fast, self.stats):
+                for part in split_group(s):
+                    run_group(part, env, fast, self.stats)
+        elif k in ("Array2DSqrt", "RedArray2D", "BlackArray2D", "Array2DSum"):
+            # no stand-alone operator: a one-statement kernel (fusion switched off)
+            from .fusion import run_group, split_group
+
+            for part in split_group(Stmt("Fused", None, (), info={"stmts": [s], "id": 0})):
+                run_group(part, env, bool(self.defines.get("hs_fast_math", False)), self.stats)
+        elif k == "ScalarSqrt":
+            env[s.dst] = np.sqrt(np.float32(env[s.args[0]]), dtype=np.float32)
+        elif k == "WarpImg2D":
+            env[s.dst] = device.warp(env[s.args[0]], env[s.args[1]], env[s.args[2]])
+        elif k == "ApplyHSPreconditioner":
+            from .cg import apply_hs_preconditioner
+
+            y0, y1 = apply_hs_preconditioner(*(env[a] for a in s.args))
+            env[s.info["dsts"][0]], env[s.info["dsts"][1]] = y0, y1
+        elif k == "HSMatrixPowers":
+            from .cg import hs_matrix_powers
+
+            steps = int(self.defines.get("STEPS", 0))
+            if steps < 1:
+                raise HMCompileError("hs_matrix_powers needs defines['STEPS'] >= 1")
+            lam = np.float32(env[s.args[0]])
+            V0, V1 = hs_matrix_powers(float(lam), *(env[a] for a in s.args[1:]), steps)
+            env[s.info["dsts"][0]], env[s.info["dsts"][1]] = V0, V1
         elif k == "Iterator":
             for _ in range(self._ub(s, env)):
                 r = self._block(s.body, env)

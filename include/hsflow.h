@@ -275,6 +275,38 @@ HS_API hs_status hs_apply_hs_preconditioner(float s2, const float *diag0, const 
                                             const float *x1, int H, int W, int ld, float *y0,
                                             float *y1, void *stream);
 
+/* ---- fused kernels for arbitrary Stencil / Array2D programs --------------------- */
+
+#define HS_FUSED_MAX_IN 16
+#define HS_FUSED_MAX_OUT 8
+#define HS_FUSED_MAX_SCALARS 64
+#define HS_FUSED_MAX_SUMS 8
+
+/* Arguments of one fused group of statements: planes share H, W and ld. */
+typedef struct hs_fused_args {
+    const float *in[HS_FUSED_MAX_IN];
+    float *out[HS_FUSED_MAX_OUT];
+    float s[HS_FUSED_MAX_SCALARS];
+    int H, W, ld;
+    int nsums;      /* sum2d reductions in the body (0..HS_FUSED_MAX_SUMS) */
+    double *sums;   /* device: nsums doubles, written */
+    int reserved[4]; /* must be zero */
+} hs_fused_args;
+
+/* Workspace (per-block partial sums) for a fused group with nsums reductions. */
+HS_API size_t hs_fused_workspace_bytes(int H, int W, int nsums);
+
+/* Runs one fused group: `body` is the CUDA C of one pixel, written with IN(k),
+ * LD(k, dx, dy) (clamp-to-edge neighbour), OUT(k) = ..., S(k), SUM(k, v) and the
+ * coordinates X, Y.  The library wraps it in its kernel skeleton, compiles it once with
+ * NVRTC for sm_100a (-fmad=false unless fast_math, so each operation rounds once, as
+ * the reference's statements do) and caches it by source.  Replaces the reference's
+ * generated-kernel path (fusion.cpp:113-303, lm.cpp:467-755, oclgen.cpp:156-185) and
+ * Array2DSum (Array2DSum.cpp:25-119).  The first call for a body compiles and loads a
+ * module: make it outside stream capture.  HS_ERR_UNSUPPORTED if NVRTC is missing. */
+HS_API hs_status hs_fused_launch(const char *body, int fast_math, const hs_fused_args *args,
+                                 void *workspace, size_t workspace_bytes, void *stream);
+
 /* ---- loss ------------------------------------------------------------------- */
 
 /* One flow field and its target for the mean end-point-error loss; du, dv receive the

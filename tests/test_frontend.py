@@ -118,3 +118,51 @@ def test_stencil_type_and_weights():
         Stencil(np.zeros(3, np.float32), [0, 1], [0, 1, 2])
     dx, dy, dt = hs_derivative_stencils()
     assert dx.ndiags == dy.ndiags == dt.ndiags == 4
+
+
+def test_fusion_groups_and_liveness():
+    """Grouping follows the stencil-read vs element-write split rule, hoists host scalar
+    statements, keeps dead intermediates out of the outputs and keeps loop-carried values."""
+    from hindemith_b200.fusion import fuse_program
+
+    src = '''
+def f(x, y, A, a):
+    p = A * x + y
+    q = p * a + 1.0
+    r = A * q
+    for i in range(3):
+        y = A * y + x
+    return r, y
+'''
+    prog = parse(src, {"x": "Array2D", "y": "Array2D", "A": "Stencil", "a": "Scalar"})
+    fuse_program(prog)
+    kinds = [s.kind for s in prog.body]
+    assert kinds.count("Fused") == 2 and "Iterator" in kinds
+    g1, g2 = [s for s in prog.body if s.kind == "Fused"]
+    # q is read by a stencil: the second group starts at `r = A * q`
+    assert [t.kind for t in g2.info["stmts"]][0] == "Stencil2DMVM"
+    assert "q" in g1.info["outputs"] and "p" not in g1.info["outputs"]
+    # the Const 1.0 was hoisted in front of the first group
+    assert prog.body.index(g1) > [s.kind for s in prog.body].index("Const")
+    loop = next(s for s in prog.body if s.kind == "Iterator")
+    (inner,) = [s for s in loop.body if s.kind == "Fused"]
+    assert "y" in inner.info["outputs"]  # loop-carried
+
+
+def test_fusion_codegen_body():
+    from hindemith_b200.fusion import codegen, fuse_program
+    from hindemith_b200 import hs_average_stencil
+
+    src = '''
+def f(x, A):
+    m = sqrt(A * x + x)
+    return m, sum2d(m)
+'''
+    prog = parse(src, {"x": "Array2D", "A": "Stencil"})
+    fuse_program(prog)
+    (g,) = [s for s in prog.body if s.kind == "Fused"]
+    body, gen = codegen(g.info["stmts"], g.info["outputs"], g.info["sums"],
+                        {"A": hs_average_stencil()})
+    assert body.count("LD(0,") == 8 and "sqrtf(" in body and "SUM(0," in body and "OUT(0)" in body
+    assert gen.inputs == ["x"]
+    assert len(gen.scalars) == 2  # the two distinct weights of the average (1/6, 1/12)
