@@ -7,7 +7,7 @@ Device API (torch CUDA tensors): ``hs_forward``, ``hs_sweeps``, ``hs_derivs``,
 The compute is libhsflow.so (hindemith_b200/_lib), a C-ABI CUDA library.
 """
 from .hindemith import defines, hm, hm_fn, state  # noqa: F401
-from .hlib import Stencil, hs_average_stencil, hs_derivative_stencils  # noqa: F401
+from .hlib import SpMat2D, Stencil, brox_offsets, hs_average_stencil, hs_derivative_stencils  # noqa: F401
 from ._lib import HSError, hs_config, make_config  # noqa: F401
 
 

@@ -36,7 +36,7 @@ import numpy as np
 from . import _lib as L
 from .hlib import Stencil, hs_average_weights
 
-ARRAY2D, STENCIL, SCALAR, ARRAY3D = "Array2D", "Stencil", "Scalar", "Array3D"
+ARRAY2D, STENCIL, SCALAR, ARRAY3D, SPMAT2D = "Array2D", "Stencil", "Scalar", "Array3D", "SpMat2D"
 _OPS = {ast.Add: "Add", ast.Sub: "Sub", ast.Mult: "Mult", ast.Div: "Div"}
 
 
@@ -77,6 +77,8 @@ def symbol_kind(obj) -> str:
 
     if isinstance(obj, Stencil) or type(obj).__name__ == "Stencil":
         return STENCIL
+    if type(obj).__name__ in ("SpMat2D", "DeviceSpMat2D"):
+        return SPMAT2D
     if isinstance(obj, np.ndarray):
         if obj.ndim == 2:
             return ARRAY2D
@@ -135,6 +137,9 @@ class _Compiler:
             name = self.fresh()
             if ka == STENCIL and kb == ARRAY2D and op == "Mult":
                 out.append(Stmt("Stencil2DMVM", name, (a, b)))
+                kind = ARRAY2D
+            elif ka == SPMAT2D and kb == ARRAY2D and op == "Mult":  # Templates.py:583-599
+                out.append(Stmt("SpmvDIA2D", name, (a, b)))
                 kind = ARRAY2D
             elif ka == ARRAY2D and kb == ARRAY2D:
                 out.append(Stmt("Array2DOp", name, (a, b), op=op))
@@ -198,10 +203,20 @@ class _Compiler:
         if fname == "warp_img2d":
             want([ARRAY2D] * 3)
             return one(ARRAY2D, "WarpImg2D")
-        if fname in ("applyHSPreconditioner", "hs_matrix_powers"):
+        if fname == "set_brox_redblack_matrix":  # Templates.py:332-350
+            want([SPMAT2D, ARRAY2D, SCALAR])
+            return one(ARRAY2D, "SetBroxRedblackMatrix")
+        if fname in ("applyHSPreconditioner", "hs_matrix_powers", "applyBroxPreconditioner",
+                     "lk_least_squares"):
             if fname == "applyHSPreconditioner":
                 want([STENCIL] + [ARRAY2D] * 5)
                 kind, res = "ApplyHSPreconditioner", ARRAY2D
+            elif fname == "applyBroxPreconditioner":  # Templates.py:377-410
+                want([SPMAT2D] + [ARRAY2D] * 5)
+                kind, res = "ApplyBroxPreconditioner", ARRAY2D
+            elif fname == "lk_least_squares":  # Templates.py:352-375
+                want([ARRAY2D] * 3)
+                kind, res = "LKLeastSquares", ARRAY2D
             else:
                 want([SCALAR, ARRAY2D, ARRAY2D, ARRAY2D, ARRAY2D])
                 kind, res = "HSMatrixPowers", ARRAY3D
@@ -284,6 +299,13 @@ class _Compiler:
                 out.append(Stmt("Return", args=names, info={"tuple": isinstance(s.value, ast.Tuple)}))
             elif isinstance(s, ast.Expr) and isinstance(s.value, ast.Constant):
                 continue  # docstring
+            elif (isinstance(s, ast.Expr) and isinstance(s.value, ast.Call)
+                  and isinstance(s.value.func, ast.Name) and s.value.func.id == "set_brox_matrix"):
+                # Templates.py:311-330: a statement that fills the matrix in place
+                args = [self.expr(a, out) for a in s.value.args]
+                if [k for _, k in args] != [SPMAT2D, ARRAY2D, SCALAR]:
+                    raise HMCompileError("set_brox_matrix(SpMat2D, Array2D, Scalar) expected")
+                out.append(Stmt("SetBroxMatrix", None, tuple(n for n, _ in args)))
             elif isinstance(s, ast.Pass):
                 continue
             else:
@@ -523,6 +545,10 @@ class Executor:
                 env[name] = device.as_plane(val)
             elif kind == SCALAR:
                 env[name] = val if isinstance(val, (np.integer, int)) else np.float32(val)
+            elif kind == SPMAT2D:
+                from .flow import DeviceSpMat2D
+
+                env[name] = val if isinstance(val, DeviceSpMat2D) else DeviceSpMat2D.from_host(val)
             else:
                 env[name] = val
         ret = self._block(self.prog.body, env)
@@ -591,6 +617,32 @@ class Executor:
             env[s.dst] = np.sqrt(np.float32(env[s.args[0]]), dtype=np.float32)
         elif k == "WarpImg2D":
             env[s.dst] = device.warp(env[s.args[0]], env[s.args[1]], env[s.args[2]])
+        elif k == "SpmvDIA2D":
+            from .flow import spmv_dia2d
+
+            env[s.dst] = spmv_dia2d(env[s.args[0]], env[s.args[1]])
+        elif k == "SetBroxMatrix":
+            from .flow import set_brox_matrix
+
+            set_brox_matrix(env[s.args[0]], env[s.args[1]], np.float32(env[s.args[2]]))
+        elif k == "SetBroxRedblackMatrix":
+            from .flow import set_brox_redblack_matrix
+
+            env[s.dst] = set_brox_redblack_matrix(env[s.args[0]], env[s.args[1]],
+                                                  np.float32(env[s.args[2]]))
+        elif k == "ApplyBroxPreconditioner":
+            from .flow import apply_brox_preconditioner
+
+            y0, y1 = apply_brox_preconditioner(*(env[a] for a in s.args))
+            env[s.info["dsts"][0]], env[s.info["dsts"][1]] = y0, y1
+        elif k == "LKLeastSquares":
+            from .flow import lk_least_squares
+
+            rad = int(self.defines.get("RADIUS", 0))
+            if rad < 1:
+                raise HMCompileError("lk_least_squares needs defines['RADIUS'] >= 1")
+            du, dv = lk_least_squares(*(env[a] for a in s.args), rad)
+            env[s.info["dsts"][0]], env[s.info["dsts"][1]] = du, dv
         elif k == "ApplyHSPreconditioner":
             from .cg import apply_hs_preconditioner
 

@@ -52,6 +52,8 @@ def _writes(s) -> List[str]:
     w += list(s.info.get("dsts", ()))
     if s.kind == "HSSweeps":
         w += [s.info["U"], s.info["V"]]
+    if s.kind in ("SetBroxMatrix", "SetBroxRedblackMatrix"):
+        w.append(s.args[0])  # fills the matrix in place
     return w
 
 

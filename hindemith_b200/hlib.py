@@ -49,6 +49,30 @@ class Stencil:
         return f"Stencil(ndiags={self.ndiags}, dtype={self.dtype})"
 
 
+class SpMat2D:
+    """A sparse 2-D grid operator in diagonal form, the reference's SpMat2D
+    (hlib.py:140-146): `data` (ndiags, H, W), one plane per diagonal, and the diagonal
+    offsets `offx`, `offy`.  On the device each diagonal is indexed by the column of its
+    entry (SpmvDIA2D.cpp:36-45, SetBroxMatrix.cpp:38-80)."""
+
+    def __init__(self, data, offx, offy):
+        self.data = data
+        self.offx = np.asarray(offx)
+        self.offy = np.asarray(offy)
+        self.ndiags, self.dim0, self.dim1 = tuple(data.shape)
+        self.dtype = data.dtype
+        if not (self.ndiags == len(self.offx) == len(self.offy)):
+            raise ValueError("SpMat2D data, offx and offy must have one entry per diagonal")
+
+    def __repr__(self):
+        return f"SpMat2D(ndiags={self.ndiags}, {self.dim0}x{self.dim1})"
+
+
+def brox_offsets():
+    """Diagonal offsets of the Brox smoothness matrix: top, left, mid, right, bottom."""
+    return (np.array([0, -1, 0, 1, 0], dtype=np.int32), np.array([-1, 0, 0, 0, 1], dtype=np.int32))
+
+
 def hs_average_stencil() -> Stencil:
     """The Horn-Schunck 3x3 average: 1/12 at the corners, 1/6 at the edges, no centre;
     taps in row-major order."""

@@ -275,6 +275,38 @@ HS_API hs_status hs_apply_hs_preconditioner(float s2, const float *diag0, const 
                                             const float *x1, int H, int W, int ld, float *y0,
                                             float *y1, void *stream);
 
+/* ---- Lucas-Kanade and Brox on the same grid substrate -------------------------- */
+
+/* LKLeastSquares.cpp:44-79: for pixels at least `radius` from the left/top border and
+ * radius+1 from the right/bottom one, the 2x2 least-squares flow over the window
+ * dx, dy in [-radius, radius) (sums from 0, dx outer), solved by Cramer's rule; du = dv = 0
+ * elsewhere and where the determinant is 0.  radius 1..16. */
+HS_API hs_status hs_lk_least_squares(const float *err, const float *Ix, const float *Iy, int H,
+                                     int W, int ld, int radius, float *du, float *dv,
+                                     void *stream);
+
+/* SetBroxMatrix.cpp:38-80 (redblack = 0) and SetBroxRedblackMatrix.cpp:38-80 (redblack = 1).
+ * `data` holds the diagonals as planes diag_stride floats apart: top, left, mid, right,
+ * bottom (5) -- or top, left, right, bottom (4) with the middle term in `adiag`.  A
+ * diagonal is indexed by the column of its entry (the neighbour); entries no pixel writes
+ * keep their values. */
+HS_API hs_status hs_set_brox_matrix(const float *psi, int H, int W, int ld, float alpha,
+                                    float *data, size_t diag_stride, int redblack, float *adiag,
+                                    void *stream);
+
+/* SpmvDIA2D.cpp:36-45: y = sum over the diagonals d (<= 16, offsets by value) whose
+ * neighbour (x + offx[d], y + offy[d]) is inside the grid of data[d] * x at that neighbour. */
+HS_API hs_status hs_spmv_dia2d(const float *data, size_t diag_stride, const int *offx,
+                               const int *offy, int ndiags, const float *x, int H, int W, int ld,
+                               float *y, void *stream);
+
+/* ApplyBroxPreconditioner.cpp:46-62: a = diag0 + mid, d = diag1 + mid, b = c = offdiag;
+ * |a d - b c| > 1e-4: the 2x2 solve; else y = x.  `mid` is the matrix's middle diagonal. */
+HS_API hs_status hs_apply_brox_preconditioner(const float *mid, const float *diag0,
+                                              const float *diag1, const float *offdiag,
+                                              const float *x0, const float *x1, int H, int W,
+                                              int ld, float *y0, float *y1, void *stream);
+
 /* ---- fused kernels for arbitrary Stencil / Array2D programs --------------------- */
 
 #define HS_FUSED_MAX_IN 16

@@ -398,3 +398,111 @@ HSO_API void hso_apply_hs_precond_f32(float s2, const float *diag0, const float 
         }
     }
 }
+
+/* ------------------------------------------------------------------ LK and Brox */
+
+/* LKLeastSquares.cpp:44-79: per pixel at least `rad` from the left/top and rad+1 from the
+ * right/bottom border, the 2x2 normal equations over the window dx, dy in [-rad, rad)
+ * (dx outer, dy inner, float accumulation from 0), solved by Cramer's rule; 0 elsewhere
+ * and where the determinant is 0. */
+HSO_API void hso_lk_least_squares_f32(const float *err, const float *Ix, const float *Iy, int H,
+                                      int W, int rad, float *du, float *dv) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const size_t i = (size_t)y * W + x;
+            float u = 0.0f, v = 0.0f;
+            if (x >= rad && y >= rad && x <= W - rad - 1 && y <= H - rad - 1) {
+                float ix2 = 0.0f, iy2 = 0.0f, ixiy = 0.0f, ixit = 0.0f, iyit = 0.0f;
+                for (int dx = -rad; dx < rad; ++dx) {
+                    for (int dy = -rad; dy < rad; ++dy) {
+                        const size_t j = (size_t)(y + dy) * W + (x + dx);
+                        const float a = Ix[j], b = Iy[j], e = err[j];
+                        ix2 += a * a;
+                        iy2 += b * b;
+                        ixiy += a * b;
+                        ixit += a * e;
+                        iyit += b * e;
+                    }
+                }
+                const float det = ix2 * iy2 - ixiy * ixiy;
+                if (det != 0.0f) {
+                    u = (ixit * iy2 - ixiy * iyit) / det;
+                    v = (ix2 * iyit - ixiy * ixit) / det;
+                }
+            }
+            du[i] = u;
+            dv[i] = v;
+        }
+    }
+}
+
+/* SetBroxMatrix.cpp:38-80 (redblack = 0: 5 diagonals top, left, mid, right, bottom) and
+ * SetBroxRedblackMatrix.cpp:38-80 (redblack = 1: 4 diagonals top, left, right, bottom and
+ * the mid term in adiag).  Diagonal d is a plane of the (ndiags, H, W) array `data`,
+ * indexed by the column of the matrix entry (the neighbour): pixel (x, y) writes
+ * top at (x, y-1), left at (x-1, y), right at (x+1, y), bottom at (x, y+1); entries no
+ * pixel writes keep their values. */
+HSO_API void hso_set_brox_matrix_f32(const float *psi, int H, int W, float alpha, float *data,
+                                     int redblack, float *adiag) {
+    const size_t P = (size_t)H * W;
+    float *top = data, *left = data + P, *mid = redblack ? adiag : data + 2 * P;
+    float *right = data + (redblack ? 2 : 3) * P, *bottom = data + (redblack ? 3 : 4) * P;
+    const float na = -alpha;
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const size_t i = (size_t)y * W + x;
+            float m = 0.0f;
+            if (y > 0) { top[i - W] = na * psi[i - W]; m += alpha * psi[i - W]; }
+            if (x > 0) { left[i - 1] = na * psi[i - 1]; m += alpha * psi[i - 1]; }
+            if (x < W - 1) { right[i + 1] = na * psi[i]; m += alpha * psi[i]; }
+            if (y < H - 1) { bottom[i + W] = na * psi[i]; m += alpha * psi[i]; }
+            mid[i] = m;
+        }
+    }
+}
+
+/* SpmvDIA2D.cpp:36-45: y = 0; for each diagonal d with (x+offx, y+offy) inside the grid,
+ * y += data[d][y+offy][x+offx] * x[y+offy][x+offx]. */
+HSO_API void hso_spmv_dia2d_f32(const float *data, const int *offx, const int *offy, int ndiags,
+                                const float *in, int H, int W, float *out) {
+    const size_t P = (size_t)H * W;
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            float acc = 0.0f;
+            for (int d = 0; d < ndiags; ++d) {
+                const int xx = x + offx[d], yy = y + offy[d];
+                if (xx >= 0 && xx < W && yy >= 0 && yy < H) {
+                    const size_t j = (size_t)yy * W + xx;
+                    acc += data[d * P + j] * in[j];
+                }
+            }
+            out[(size_t)y * W + x] = acc;
+        }
+    }
+}
+
+/* ApplyBroxPreconditioner.cpp:46-62: a = diag0 + mid, d = diag1 + mid (mid = the
+ * matrix's middle diagonal at the pixel), det = a d - b c; |det| > 1e-4: the 2x2 solve,
+ * else y = x. */
+HSO_API void hso_apply_brox_precond_f32(const float *mid, const float *diag0, const float *diag1,
+                                        const float *offdiag, const float *x0, const float *x1,
+                                        int H, int W, float *y0, float *y1) {
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < H; ++y) {
+        for (int x = 0; x < W; ++x) {
+            const size_t i = (size_t)y * W + x;
+            const float a = diag0[i] + mid[i], d = diag1[i] + mid[i];
+            const float b = offdiag[i], c = offdiag[i], e = x0[i], f = x1[i];
+            const float det = a * d - b * c;
+            if (fabsf(det) > 1e-4f) {
+                y0[i] = (e * d - b * f) / det;
+                y1[i] = (-c * e + a * f) / det;
+            } else {
+                y0[i] = e;
+                y1[i] = f;
+            }
+        }
+    }
+}

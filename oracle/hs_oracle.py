@@ -181,6 +181,11 @@ def lib():
                                                c_int, f32p, f32p]
         L.hso_apply_hs_precond_f32.argtypes = [c_float, f32p, f32p, f32p, f32p, f32p, c_int,
                                                c_int, f32p, f32p]
+        L.hso_lk_least_squares_f32.argtypes = [f32p, f32p, f32p, c_int, c_int, c_int, f32p, f32p]
+        L.hso_set_brox_matrix_f32.argtypes = [f32p, c_int, c_int, c_float, f32p, c_int, f32p]
+        L.hso_spmv_dia2d_f32.argtypes = [f32p, i32p, i32p, c_int, f32p, c_int, c_int, f32p]
+        L.hso_apply_brox_precond_f32.argtypes = [f32p, f32p, f32p, f32p, f32p, f32p, c_int, c_int,
+                                                 f32p, f32p]
         for name in ("hso_hs_sweeps_f32", "hso_hs_sweeps_f64", "hso_hs_forward_f32",
                      "hso_hs_forward_f64"):
             getattr(L, name).restype = c_int
@@ -282,6 +287,50 @@ def c_apply_hs_precond(s2, diag0, diag1, offdiag, x0, x1):
     y0, y1 = np.empty_like(x0), np.empty_like(x0)
     lib().hso_apply_hs_precond_f32(float(np.float32(s2)), diag0, diag1, offdiag, x0, x1, H, W, y0, y1)
     return y0, y1
+
+
+def c_lk_least_squares(err, Ix, Iy, rad):
+    """LKLeastSquares.cpp:44-79 in FP32 -> du, dv."""
+    err, Ix, Iy = _c32(err), _c32(Ix), _c32(Iy)
+    H, W = err.shape
+    du, dv = np.empty_like(err), np.empty_like(err)
+    lib().hso_lk_least_squares_f32(err, Ix, Iy, H, W, int(rad), du, dv)
+    return du, dv
+
+
+def c_set_brox_matrix(psi, alpha, data, redblack=False):
+    """SetBroxMatrix.cpp / SetBroxRedblackMatrix.cpp in FP32: updates a copy of `data`
+    (ndiags, H, W) and returns it (and the mid term for the red-black form)."""
+    psi = _c32(psi)
+    H, W = psi.shape
+    data = _c32(data).copy()
+    adiag = np.zeros((H, W), np.float32)
+    lib().hso_set_brox_matrix_f32(psi, H, W, float(np.float32(alpha)), data, 1 if redblack else 0, adiag)
+    return (data, adiag) if redblack else data
+
+
+def c_spmv_dia2d(data, offx, offy, x):
+    """SpmvDIA2D.cpp:36-45 in FP32."""
+    data, x = _c32(data), _c32(x)
+    H, W = x.shape
+    out = np.empty_like(x)
+    ox = np.ascontiguousarray(offx, dtype=np.int32)
+    oy = np.ascontiguousarray(offy, dtype=np.int32)
+    lib().hso_spmv_dia2d_f32(data, ox, oy, len(ox), x, H, W, out)
+    return out
+
+
+def c_apply_brox_precond(mid, diag0, diag1, offdiag, x0, x1):
+    """ApplyBroxPreconditioner.cpp:46-62 in FP32."""
+    mid, diag0, diag1, offdiag, x0, x1 = (_c32(a) for a in (mid, diag0, diag1, offdiag, x0, x1))
+    H, W = x0.shape
+    y0, y1 = np.empty_like(x0), np.empty_like(x0)
+    lib().hso_apply_brox_precond_f32(mid, diag0, diag1, offdiag, x0, x1, H, W, y0, y1)
+    return y0, y1
+
+
+BROX_OFFX = np.array([0, -1, 0, 1, 0], np.int32)   # top, left, mid, right, bottom
+BROX_OFFY = np.array([-1, 0, 0, 0, 1], np.int32)
 
 
 def hs_normal_matrix(lam, Ix, Iy):

@@ -25,6 +25,8 @@ Fixtures (tests/golden/*.npz):
   hs_*.npz       : I0, I1, alpha2, sweeps, Ix, Iy, It, u, v   (hs_programs.hs_jacobi)
   warp_*.npz     : src, ox, oy, out                 (warp_img2d, integer offsets)
   precond_*.npz  : s2, d0_i, d1_i, od_i, x0_i, x1_i, y0_i, y1_i   (applyHSPreconditioner)
+  brox.npz       : alpha, psi_i, x_i, ax_i (set_brox_matrix then A*x), mid_i, d0_i, d1_i,
+                   od_i, x0_i, x1_i, y0_i, y1_i (applyBroxPreconditioner)
 """
 from __future__ import annotations
 
@@ -168,6 +170,33 @@ def main(ref_root: str):
                          f"y1_{i}": np.asarray(y1, np.float32)})
         np.savez_compressed(os.path.join(out_dir, f"precond_{cname}.npz"),
                             s2=np.float32(0.25 * scale), n=np.int32(4), **arrs)
+    # Brox: set_brox_matrix (hlib.py:71-81) then the SpMat2D product (hlib.py:148-164),
+    # and applyBroxPreconditioner (hlib.py:49-69).  hlib stores each diagonal at the row of
+    # the matrix entry, the device templates at its column; A*x agrees between the two.
+    brng = np.random.Generator(np.random.PCG64(13))
+    arrs = {}
+    shapes = [(1, 1), (1, 6), (5, 1), (9, 14)]
+    offx = np.array([0, -1, 0, 1, 0])
+    offy = np.array([-1, 0, 0, 0, 1])
+    for i, (H, W) in enumerate(shapes):
+        psi = brng.uniform(0.1, 1.0, (H, W)).astype(np.float32)
+        x = brng.standard_normal((H, W)).astype(np.float32)
+        Am = hl.SpMat2D(np.zeros((5, H, W), np.float32), offx, offy)
+        alpha = np.float32(0.75)
+        hl.set_brox_matrix(Am, psi, alpha)
+        ax = Am * x
+        d0 = brng.uniform(0.1, 1.0, (H, W)).astype(np.float32)
+        d1 = brng.uniform(0.1, 1.0, (H, W)).astype(np.float32)
+        od = brng.uniform(-0.05, 0.05, (H, W)).astype(np.float32)
+        x0 = brng.standard_normal((H, W)).astype(np.float32)
+        x1 = brng.standard_normal((H, W)).astype(np.float32)
+        y0, y1 = hl.applyBroxPreconditioner(Am, d0, d1, od, x0, x1)
+        arrs.update({f"psi_{i}": psi, f"x_{i}": x, f"ax_{i}": np.asarray(ax, np.float32),
+                     f"mid_{i}": Am.data[2].copy(), f"d0_{i}": d0, f"d1_{i}": d1, f"od_{i}": od,
+                     f"x0_{i}": x0, f"x1_{i}": x1, f"y0_{i}": np.asarray(y0, np.float32),
+                     f"y1_{i}": np.asarray(y1, np.float32)})
+    np.savez_compressed(os.path.join(out_dir, "brox.npz"), alpha=np.float32(0.75),
+                        n=np.int32(len(shapes)), **arrs)
     print("wrote fixtures to", out_dir)
 
 

@@ -179,3 +179,17 @@ def test_cg_family_argument_checks():
     assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, P, P, 8, 6, 6, P, P, None) == L.HS_ERR_ALIGNMENT
     assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, P, P, 0, 8, 8, P, P, None) == L.HS_ERR_INVALID_ARG
     assert lib.hs_apply_hs_preconditioner(0.25, P, P, P, fake_ptr(8), P, 8, 8, 8, P, P, None) == L.HS_ERR_ALIGNMENT
+
+
+def test_lk_brox_argument_checks():
+    lib = L.lib()
+    P = fake_ptr()
+    assert lib.hs_lk_least_squares(P, P, P, 8, 8, 8, 0, P, P, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_lk_least_squares(P, P, P, 8, 8, 8, 17, P, P, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_lk_least_squares(P, None, P, 8, 8, 8, 2, P, P, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_set_brox_matrix(P, 8, 8, 8, 1.0, P, 32, 0, None, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_set_brox_matrix(P, 8, 8, 8, 1.0, P, 64, 1, None, None) == L.HS_ERR_INVALID_ARG
+    ox = (ctypes.c_int * 17)()
+    assert lib.hs_spmv_dia2d(P, 64, ox, ox, 17, P, 8, 8, 8, fake_ptr(256), None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_spmv_dia2d(P, 64, ox, ox, 5, P, 8, 8, 8, P, None) == L.HS_ERR_INVALID_ARG  # x == y
+    assert lib.hs_apply_brox_preconditioner(P, P, P, P, P, P, 8, 8, 8, P, fake_ptr(2), None) == L.HS_ERR_ALIGNMENT

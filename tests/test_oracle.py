@@ -229,3 +229,42 @@ def test_matrix_powers_oracle_matches_sparse_operator():
             got = np.concatenate([V0[s].ravel(), V1[s].ravel()]) / max(np.abs(x).max(), 1e-30)
             assert np.abs(got - ref).max() < 1e-5
             x = M @ x
+
+
+def test_brox_oracle_matches_reference_golden():
+    """set_brox_matrix + SpMat2D product and applyBroxPreconditioner (hlib.py:49-81,
+    148-164) vs the restatement of the device templates: bit-identical.  (hlib indexes each
+    diagonal by the row of its entry, the device templates by its column; the product is
+    the same either way.)"""
+    g = golden("brox.npz")
+    for i in range(int(g["n"])):
+        H, W = g[f"psi_{i}"].shape
+        data = O.c_set_brox_matrix(g[f"psi_{i}"], g["alpha"], np.zeros((5, H, W), np.float32))
+        assert_bitexact(O.c_spmv_dia2d(data, O.BROX_OFFX, O.BROX_OFFY, g[f"x_{i}"]), g[f"ax_{i}"])
+        assert_bitexact(data[2], g[f"mid_{i}"])
+        y0, y1 = O.c_apply_brox_precond(data[2], g[f"d0_{i}"], g[f"d1_{i}"], g[f"od_{i}"],
+                                        g[f"x0_{i}"], g[f"x1_{i}"])
+        assert_bitexact(y0, g[f"y0_{i}"])
+        assert_bitexact(y1, g[f"y1_{i}"])
+
+
+def test_lk_oracle_matches_float64_restatement():
+    """The LKLeastSquares restatement against an independent FP64 NumPy evaluation of the
+    same template (window [-r, r)^2, interior rule): parity unpinned against the reference
+    itself, whose NumPy lk_least_squares (hlib.py:86-118) uses a (2r+1)^2 window."""
+    rng = np.random.default_rng(9)
+    for (H, W, r) in ((12, 15, 2), (20, 9, 3), (5, 5, 2)):
+        err, Ix, Iy = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(3))
+        du, dv = O.c_lk_least_squares(err, Ix, Iy, r)
+        rdu, rdv = np.zeros((H, W)), np.zeros((H, W))
+        for y in range(r, H - r):
+            for x in range(r, W - r):
+                a = Ix[y - r:y + r, x - r:x + r].astype(np.float64)
+                b = Iy[y - r:y + r, x - r:x + r].astype(np.float64)
+                e = err[y - r:y + r, x - r:x + r].astype(np.float64)
+                M = np.array([[(a * a).sum(), (a * b).sum()], [(a * b).sum(), (b * b).sum()]])
+                rhs = np.array([(a * e).sum(), (b * e).sum()])
+                rdu[y, x], rdv[y, x] = np.linalg.solve(M, rhs)
+        scale = max(np.abs(rdu).max(), np.abs(rdv).max(), 1e-6)
+        assert np.abs(du - rdu).max() < 1e-4 * scale
+        assert np.abs(dv - rdv).max() < 1e-4 * scale
