@@ -31,7 +31,7 @@ namespace hs {
 constexpr int kMaxTrainPairs = 32;
 constexpr int kMaxTB = 5;
 constexpr int kAdjMaxDepth = 4;     // deepest adjoint pass the backward plans
-constexpr int kAdjItemsPerSm = 12;  // adjoint work items (warps) per SM and launch
+constexpr int kAdjItemsPerSmMax = 16;  // adjoint work items (warps) per SM and launch, at most
 constexpr int kMinStripCols = 52;   // narrowest adjoint strip (depth <= 5): 64 less 6 each side
 
 // ------------------------------------------------------------------ table-driven pass
@@ -320,8 +320,11 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
     if (it.lane == 0) P.a2part[local] += d;
 }
 
+// resident CTAs per SM the register budget is sized for: depth <= 3 fits 4 (16 warps/SM)
+constexpr int adj_min_blocks(int TB) { return TB <= 3 ? 4 : 3; }
+
 template <int TB>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, 3)
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, adj_min_blocks(TB))
     hs_adjoint_pass_kernel(const __grid_constant__ AdjTable tab) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -495,7 +498,7 @@ static hs_status train_layout(const hs_train_pair *pairs, int n, int iters, int 
     // items of one pair in one adjoint launch <= (all rows / rows per item) + its strips
     int maxW = 1;
     for (int i = 0; i < n; ++i) maxW = std::max(maxW, pairs[i].W);
-    L.nslots = sm_count() * kAdjItemsPerSm + (maxW + kMinStripCols - 1) / kMinStripCols;
+    L.nslots = sm_count() * kAdjItemsPerSmMax + (maxW + kMinStripCols - 1) / kMinStripCols;
     L.total = L.partials_off + round_up((size_t)n * L.nslots * sizeof(double), 256);
     return HS_OK;
 }
@@ -672,8 +675,10 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
             done += t;
         }
         // 2. adjoint sweeps j = nsw-1 .. 0 in passes of up to TB
-        for (int jhi = nsw; jhi > 0;) {
-            const int tb = std::min(TB, jhi);
+        // the interval's sweeps in ceil(nsw / TB) passes of balanced depth (10 = 4 + 3 + 3)
+        const int npass = (nsw + TB - 1) / TB;
+        for (int jhi = nsw, q = 0; jhi > 0; ++q) {
+            const int tb = (jhi + (npass - q) - 1) / (npass - q);
             AdjTable tab;
             memset(&tab, 0, sizeof(tab));
             tab.npairs = n;
@@ -681,7 +686,7 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
             tab.wc = rc.wc;
             long rows = 0;
             for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
-            const long target = (long)sm_count() * kAdjItemsPerSm;
+            const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
             int Lr = (int)std::max(1L, (rows + target - 1) / target);
             Lr = std::max(Lr, std::max(8, 2 * tb));
             tab.item_prefix[0] = 0;
