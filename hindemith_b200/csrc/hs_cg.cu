@@ -60,16 +60,78 @@ __device__ __forceinline__ void mp_cell(const float *u, const float *v, const fl
     }
 }
 
-// `depth` (<= D) powers: V[s0+1 .. s0+depth] from V[s0].  Loads and stores move 16-byte
-// groups (the tile's first column is a multiple of 4, rows start 16-byte aligned); tile cells
-// outside the image load as 0 and are never read by an in-image cell (the neighbour tests
-// skip them).
+// One power over the tile region [x0, x0+SX) x [y0, y0+SY) (tile coordinates), flattened
+// over the CTA's threads.  INTERIOR: the whole tile lies at least one cell inside the image,
+// so every computed cell has its four neighbours and no test is needed.
+template <int EX, int SX, int SY, bool INTERIOR>
+__device__ __forceinline__ void mp_region(const float *u, const float *v, const float *sIx,
+                                          const float *sIy, float *uo, float *vo, int x0, int y0,
+                                          int tx0, int ty0, int H, int W, float lam) {
+    for (int k = threadIdx.x; k < SX * SY; k += kMpThreads) {
+        const int cy = y0 + k / SX, cx = x0 + k % SX;
+        const int c = cy * EX + cx;
+        float ur, vr;
+        if constexpr (INTERIOR) {
+            mp_cell(u, v, sIx, sIy, c, EX, 1, 1, 3, 3, lam, ur, vr);  // all neighbours present
+        } else {
+            const int x = tx0 + cx, y = ty0 + cy;
+            if (x < 0 || x >= W || y < 0 || y >= H) continue;
+            mp_cell(u, v, sIx, sIy, c, EX, x, y, H, W, lam, ur, vr);
+        }
+        uo[c] = ur;
+        vo[c] = vr;
+    }
+}
+
+// Power T of a pass of D (T = 1 .. D, unrolled at compile time): compute it over the
+// region still needed by the later powers, then store its core.
+template <int D, int T>
+__device__ __forceinline__ void mp_power(float *sIx, float *sIy, float *su0, float *sv0, float *su1,
+                                         float *sv1, bool interior, int tx0, int ty0, int H, int W,
+                                         int ld, float lam, float *V0, float *V1, size_t pstride) {
+    constexpr int EX = MpGeo<D>::EX;
+    constexpr int M = D - T;  // power T is needed within M cells of the core
+    constexpr int SX = kMpTX + 2 * M, SY = kMpTY + 2 * M;
+    constexpr bool odd = T & 1;
+    const float *u = odd ? su0 : su1, *v = odd ? sv0 : sv1;
+    float *uo = odd ? su1 : su0, *vo = odd ? sv1 : sv0;
+    if (interior)
+        mp_region<EX, SX, SY, true>(u, v, sIx, sIy, uo, vo, kMpHX - M, D - M, tx0, ty0, H, W, lam);
+    else
+        mp_region<EX, SX, SY, false>(u, v, sIx, sIy, uo, vo, kMpHX - M, D - M, tx0, ty0, H, W, lam);
+    __syncthreads();
+    // store the core (the next power reads uo as well and writes the other buffer)
+    float *out0 = V0 + (size_t)T * pstride, *out1 = V1 + (size_t)T * pstride;
+    for (int k = threadIdx.x; k < (kMpTX / 4) * kMpTY; k += kMpThreads) {
+        const int gx = k % (kMpTX / 4), cy = D + k / (kMpTX / 4);
+        const int x = tx0 + kMpHX + 4 * gx, y = ty0 + cy;
+        if (x >= W || y >= H) continue;
+        const int c = cy * EX + kMpHX + 4 * gx;
+        const size_t o = (size_t)y * ld + x;
+        if (x + 4 <= W) {
+            *reinterpret_cast<float4 *>(out0 + o) = *reinterpret_cast<const float4 *>(uo + c);
+            *reinterpret_cast<float4 *>(out1 + o) = *reinterpret_cast<const float4 *>(vo + c);
+        } else {
+            for (int j = 0; j < W - x; ++j) {
+                out0[o + j] = uo[c + j];
+                out1[o + j] = vo[c + j];
+            }
+        }
+    }
+    if constexpr (T < D)
+        mp_power<D, T + 1>(sIx, sIy, su0, sv0, su1, sv1, interior, tx0, ty0, H, W, ld, lam, V0, V1,
+                           pstride);
+}
+
+// D powers: V[s0+1 .. s0+D] from V[s0].  Loads and stores move 16-byte groups (the tile's
+// first column is a multiple of 4, rows start 16-byte aligned); tile cells outside the image
+// load as 0 and are never read by an in-image cell (the neighbour tests skip them).
 template <int D>
 __global__ void __launch_bounds__(kMpThreads) mp_pass_kernel(float lam, const float *__restrict__ Ix,
                                                              const float *__restrict__ Iy,
                                                              const float *u_in, const float *v_in,
                                                              float *V0, float *V1, size_t pstride,
-                                                             int H, int W, int ld, int depth) {
+                                                             int H, int W, int ld) {
     using G = MpGeo<D>;
     constexpr int EX = G::EX, EY = G::EY, GX = EX / 4;
     extern __shared__ float4 sm4[];
@@ -77,6 +139,7 @@ __global__ void __launch_bounds__(kMpThreads) mp_pass_kernel(float lam, const fl
     float *sIx = sm, *sIy = sm + G::N;
     float *su0 = sm + 2 * G::N, *sv0 = sm + 3 * G::N, *su1 = sm + 4 * G::N, *sv1 = sm + 5 * G::N;
     const int tx0 = blockIdx.x * kMpTX - kMpHX, ty0 = blockIdx.y * kMpTY - D;
+    const bool interior = tx0 >= 1 && ty0 >= 1 && tx0 + EX <= W - 1 && ty0 + EY <= H - 1;
     for (int c = threadIdx.x; c < GX * EY; c += kMpThreads) {
         const int gx = c % GX, cy = c / GX;
         const int x = tx0 + 4 * gx, y = ty0 + cy;
@@ -95,49 +158,7 @@ __global__ void __launch_bounds__(kMpThreads) mp_pass_kernel(float lam, const fl
         *reinterpret_cast<float4 *>(sv0 + k) = q;
     }
     __syncthreads();
-    for (int t = 1; t <= depth; ++t) {
-        const bool odd = t & 1;
-        const float *u = odd ? su0 : su1, *v = odd ? sv0 : sv1;
-        float *uo = odd ? su1 : su0, *vo = odd ? sv1 : sv0;
-        // power t is needed within depth - t cells of the core
-        const int m = depth - t;
-        const int x0 = kMpHX - m, sx = kMpTX + 2 * m;
-        const int y0 = D - m, sy = kMpTY + 2 * m;
-        // warp lanes walk a row (consecutive cells), the 8 warps walk rows
-        const int lane = threadIdx.x & 31, wy = threadIdx.x >> 5;
-        for (int cy = y0 + wy; cy < y0 + sy; cy += kMpThreads / 32) {
-            const int y = ty0 + cy;
-            if (y < 0 || y >= H) continue;
-            for (int cx = x0 + lane; cx < x0 + sx; cx += 32) {
-                const int x = tx0 + cx;
-                if (x < 0 || x >= W) continue;
-                const int c = cy * EX + cx;
-                float ur, vr;
-                mp_cell(u, v, sIx, sIy, c, EX, x, y, H, W, lam, ur, vr);
-                uo[c] = ur;
-                vo[c] = vr;
-            }
-        }
-        __syncthreads();
-        // store the core of power t (the next power reads uo too and writes the other buffer)
-        float *out0 = V0 + (size_t)t * pstride, *out1 = V1 + (size_t)t * pstride;
-        for (int k = threadIdx.x; k < (kMpTX / 4) * kMpTY; k += kMpThreads) {
-            const int gx = k % (kMpTX / 4), cy = D + k / (kMpTX / 4);
-            const int x = tx0 + kMpHX + 4 * gx, y = ty0 + cy;
-            if (x >= W || y >= H) continue;
-            const int c = cy * EX + kMpHX + 4 * gx;
-            const size_t o = (size_t)y * ld + x;
-            if (x + 4 <= W) {
-                *reinterpret_cast<float4 *>(out0 + o) = *reinterpret_cast<const float4 *>(uo + c);
-                *reinterpret_cast<float4 *>(out1 + o) = *reinterpret_cast<const float4 *>(vo + c);
-            } else {
-                for (int j = 0; j < W - x; ++j) {
-                    out0[o + j] = uo[c + j];
-                    out1[o + j] = vo[c + j];
-                }
-            }
-        }
-    }
+    mp_power<D, 1>(sIx, sIy, su0, sv0, su1, sv1, interior, tx0, ty0, H, W, ld, lam, V0, V1, pstride);
 }
 
 __device__ __forceinline__ void precond_px(float s2, float a, float d, float b, float e, float f,
@@ -198,7 +219,7 @@ __global__ void __launch_bounds__(256) precond_kernel(float s2, const float *__r
 template <int D>
 static hs_status launch_mp(float lam, const float *Ix, const float *Iy, const float *u,
                            const float *v, float *V0, float *V1, size_t pstride, int H, int W,
-                           int ld, int depth, cudaStream_t s) {
+                           int ld, cudaStream_t s) {
     static bool attr[64] = {};
     int dev = 0;
     HS_CUDA_CHECK(cudaGetDevice(&dev));
@@ -209,7 +230,7 @@ static hs_status launch_mp(float lam, const float *Ix, const float *Iy, const fl
     }
     const dim3 grid((unsigned)((W + kMpTX - 1) / kMpTX), (unsigned)((H + kMpTY - 1) / kMpTY));
     mp_pass_kernel<D><<<grid, kMpThreads, MpGeo<D>::smem_bytes, s>>>(lam, Ix, Iy, u, v, V0, V1,
-                                                                      pstride, H, W, ld, depth);
+                                                                      pstride, H, W, ld);
     HS_LAUNCH_CHECK("mp_pass_kernel");
     return HS_OK;
 }
@@ -242,11 +263,11 @@ hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const fl
     for (int s0 = 0; s0 + 1 < steps; s0 += depth) {
         const int d = std::min(depth, steps - 1 - s0);
         float *b0 = V0 + (size_t)s0 * power_stride, *b1 = V1 + (size_t)s0 * power_stride;
-        switch (depth) {
-            case 1: st = launch_mp<1>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, d, s); break;
-            case 2: st = launch_mp<2>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, d, s); break;
-            case 3: st = launch_mp<3>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, d, s); break;
-            default: st = launch_mp<4>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, d, s); break;
+        switch (d) {  // this pass's depth
+            case 1: st = launch_mp<1>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
+            case 2: st = launch_mp<2>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
+            case 3: st = launch_mp<3>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
+            default: st = launch_mp<4>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
         }
         if (st != HS_OK) return st;
     }
