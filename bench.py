@@ -383,6 +383,79 @@ def measure_pyramid(args, rank, flush):
             "input_bytes": int(base)}
 
 
+def flow_magnitude(I0, I1, Dx, Dy, Dt, eps):
+    """A generic @hm program (not the HS loop): derivative stencils, gradient magnitude,
+    its normalisation by the plane sum."""
+    Ix = Dx * I0 + Dx * I1
+    Iy = Dy * I0 + Dy * I1
+    It = Dt * I1 - Dt * I0
+    m = sqrt(Ix * Ix + Iy * Iy + eps)  # noqa: F821 (the @hm surface's sqrt)
+    return m / sum2d(m), It  # noqa: F821
+
+
+def measure_fusion_flow(args, rank, flush, peak):
+    """Generic fusion (the program above at 1920x1080, fused vs one operator per statement),
+    Lucas-Kanade (1920x1080, radius 5) and the Brox pieces (2048x2048)."""
+    import numpy as np
+    import torch
+
+    from hindemith_b200 import SpMat2D, brox_offsets, hm, hs_derivative_stencils
+    from hindemith_b200 import device as D
+    from hindemith_b200 import flow as FL
+    from hindemith_b200 import hindemith as HM
+
+    stream = torch.cuda.current_stream()
+    k = max(1, args.steps)
+    g = torch.Generator(device="cuda")
+    g.manual_seed(11 + rank)
+    H, W = 1080, 1920
+    I0, I1 = (torch.rand((H, W), device="cuda", generator=g) for _ in range(2))
+    Dx, Dy, Dt = hs_derivative_stencils()
+    out = {}
+    f = hm(flow_magnitude)
+    kw = dict(I0=I0, I1=I1, Dx=Dx, Dy=Dy, Dt=Dt, eps=np.float32(1e-3))
+    old = dict(HM.defines)
+    try:
+        for fuse in (True, False):
+            HM.defines["hs_fuse"] = fuse
+            t = timed_events(lambda: f(**kw), k, 3, flush, stream, "timed_fusion")
+            out["fused_ms" if fuse else "unfused_ms"] = t / k * 1e3
+            if fuse:
+                out["fused_kernels_per_call"] = HM.state["last_stats"].get("fused_launches", 0)
+    finally:
+        HM.defines.clear()
+        HM.defines.update(old)
+    # fused bytes: read I0, I1 (twice: two groups read what they need) + write It, n, m once
+    out["fused_bytes_per_px"] = 4 * (2 + 1 + 1 + 1 + 1)
+    out["fused_gbs"] = out["fused_bytes_per_px"] * H * W / (out["fused_ms"] / 1e3) / 1e9
+    err, Ix, Iy = D.empty_planes(3, H, W)
+    for p in (err, Ix, Iy):
+        p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
+    t = timed_events(lambda: FL.lk_least_squares(err, Ix, Iy, 5), k, 3, flush, stream, "timed_lk")
+    lk_flops = H * W * (2 * 5) ** 2 * 10
+    out["lk"] = {"workload": "lk_least_squares_1920x1080_radius5", "ms": t / k * 1e3,
+                 "gflops": lk_flops * k / t / 1e9, "bound": "fp32 issue"}
+    Hb = Wb = 2048
+    psi, x, d0, d1, od = D.empty_planes(5, Hb, Wb)
+    for p in (psi, x, d0, d1, od):
+        p.copy_(torch.rand((Hb, Wb), device="cuda", generator=g) + 0.1)
+    offx, offy = brox_offsets()
+    A = FL.DeviceSpMat2D.from_host(SpMat2D(np.zeros((5, Hb, Wb), np.float32), offx, offy))
+    t_set = timed_events(lambda: FL.set_brox_matrix(A, psi, 0.5), k, 3, flush, stream, "timed_brox_set")
+    t_mv = timed_events(lambda: FL.spmv_dia2d(A, x), k, 3, flush, stream, "timed_spmv")
+    t_pc = timed_events(lambda: FL.apply_brox_preconditioner(A, d0, d1, od, x, psi), k, 3, flush,
+                        stream, "timed_brox_precond")
+    px = Hb * Wb
+    out["brox"] = {"workload": "brox_2048x2048",
+                   "set_matrix": {"ms": t_set / k * 1e3, "gbs": 24 * px * k / t_set / 1e9},
+                   "spmv_dia2d": {"ms": t_mv / k * 1e3, "gbs": 28 * px * k / t_mv / 1e9},
+                   "preconditioner": {"ms": t_pc / k * 1e3, "gbs": 36 * px * k / t_pc / 1e9},
+                   "peak_gbs": peak}
+    out["workload"] = ("flow_magnitude_1920x1080 (@hm call end to end, including the host "
+                       "read of sum2d; fused vs one operator per statement)")
+    return out
+
+
 def measure_cg(args, rank, flush, peak):
     """Horn-Schunck as a linear system at 2048x2048: 9 Krylov powers of the HS operator
     (hs_matrix_powers, 4 powers per pass) and one block-Jacobi preconditioner application,
@@ -646,6 +719,7 @@ def main():
         line["fwd_bwd"] = measure_train(args, rank, flush)
     if world == 1 and not args.no_cg and not args.shape:
         line["cg"] = measure_cg(args, rank, flush, peak)
+        line["fusion_lk_brox"] = measure_fusion_flow(args, rank, flush, peak)
     if world == 1 and not args.no_pyramid and not args.shape:
         line["pyramid"] = measure_pyramid(args, rank, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -255,12 +255,22 @@ def run_group(stmt, env, fast_math: bool, stats: Dict[str, int]) -> bool:
     from . import device as D
 
     info = stmt.info
-    try:
-        body, g = codegen(info["stmts"], info["outputs"], info["sums"], env)
-    except _TooBig:
-        stats["fused_fallback"] = stats.get("fused_fallback", 0) + 1
-        return False
-    planes = D._same_layout(*(env[n] for n in g.inputs)) if g.inputs else ()
+    # the generated body depends on the stencils' taps and the scalar operands' values only
+    # (inputs, outputs and their order are fixed by the statements): cache it per value set
+    key = _value_signature(info["stmts"], env)
+    cache = info.setdefault("codegen_cache", {})
+    hit = cache.get(key)
+    if hit is None:
+        try:
+            body, g = codegen(info["stmts"], info["outputs"], info["sums"], env)
+        except _TooBig:
+            stats["fused_fallback"] = stats.get("fused_fallback", 0) + 1
+            return False
+        hit = (body.encode(), list(g.inputs), list(g.scalars))
+        if len(cache) < 64:
+            cache[key] = hit
+    body_b, inputs, scalars = hit
+    planes = D._same_layout(*(env[n] for n in inputs)) if inputs else ()
     if planes:
         H, W = planes[0].shape
         ld = planes[0].stride(0)
@@ -276,7 +286,7 @@ def run_group(stmt, env, fast_math: bool, stats: Dict[str, int]) -> bool:
     outs = torch.empty((max(1, len(info["outputs"])), H, ld), dtype=torch.float32, device=dev)
     for j in range(len(info["outputs"])):
         args.out[j] = outs[j].data_ptr()
-    for j, v in enumerate(g.scalars):
+    for j, v in enumerate(scalars):
         args.s[j] = v
     args.H, args.W, args.ld = H, W, ld
     nsums = len(info["sums"])
@@ -287,7 +297,7 @@ def run_group(stmt, env, fast_math: bool, stats: Dict[str, int]) -> bool:
         sums_dev = torch.empty(nsums, dtype=torch.float64, device=dev)
         args.sums = sums_dev.data_ptr()
         ws = torch.empty(int(lib.hs_fused_workspace_bytes(H, W, nsums)), dtype=torch.uint8, device=dev)
-    L.check(lib.hs_fused_launch(body.encode(), 1 if fast_math else 0, ctypes.byref(args),
+    L.check(lib.hs_fused_launch(body_b, 1 if fast_math else 0, ctypes.byref(args),
                                 D.ptr(ws) if ws is not None else None,
                                 ws.numel() if ws is not None else 0, D.stream_handle()),
             "hs_fused_launch")
@@ -299,6 +309,19 @@ def run_group(stmt, env, fast_math: bool, stats: Dict[str, int]) -> bool:
         for j, name in enumerate(info["sums"]):
             env[name] = np.float32(vals[j])
     return True
+
+
+def _value_signature(stmts, env) -> tuple:
+    parts = []
+    for t in stmts:
+        if t.kind == "Stencil2DMVM":
+            w, ox, oy = env[t.args[0]].taps()
+            parts.append((w.tobytes(), ox.tobytes(), oy.tobytes()))
+        elif t.kind == "Array2DScalarOp":
+            parts.append(np.float32(env[t.args[1]]).tobytes())
+        elif t.kind == "ScalarArray2DOp":
+            parts.append(np.float32(env[t.args[0]]).tobytes())
+    return tuple(parts)
 
 
 def split_group(stmt):

@@ -70,8 +70,10 @@ class hm_fn:
         if args:
             raise HMCompileError("@hm functions take keyword arguments only")
         ex = self.compile(**kwargs)
+        before = dict(ex.stats)
         out = ex.run(kwargs)
-        state["last_stats"] = dict(ex.stats)
+        # counts of this call alone
+        state["last_stats"] = {k: v - before.get(k, 0) for k, v in ex.stats.items()}
         return out
 
 
