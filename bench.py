@@ -41,6 +41,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--sweeps-per-pass", type=int, default=0, help="0 = autotuned")
+    ap.add_argument("--layout", type=int, default=0,
+                    help="with --sweeps-per-pass: 1 = 2 columns per lane, 2 = 4, 0 = by image size")
     ap.add_argument("--exact", action="store_true", help="bit-exact operation order")
     ap.add_argument("--cpu-sample-sweeps", type=int, default=20)
     ap.add_argument("--shape", default="", help="HxW override (profiling cases)")
@@ -52,6 +54,8 @@ def parse_args():
     ap.add_argument("--batch-sweeps-per-pass", type=int, default=0,
                     help="batched leg: sweeps per pass (0 = autotuned with the rows per tile)")
     ap.add_argument("--batch-rows", type=int, default=0, help="batched leg: rows per tile")
+    ap.add_argument("--batch-layout", type=int, default=0,
+                    help="batched leg: 1 = 2 columns per lane, 2 = 4, 0 = by pair size")
     ap.add_argument("--no-train", action="store_true")
     ap.add_argument("--train-sweeps-per-pass", type=int, default=5)
     ap.add_argument("--no-pyramid", action="store_true")
@@ -227,10 +231,11 @@ def measure_batched(args, rank, flush, peak):
         sp.seed += 100 * rank
     shape = [(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs]
     if args.batch_sweeps_per_pass > 0:
-        T, rows = args.batch_sweeps_per_pass, args.batch_rows
+        T, rows, layout = args.batch_sweeps_per_pass, args.batch_rows, args.batch_layout
     else:
-        T, rows = best_batch_config(shape, fast_math=not args.exact)
-    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=rows, fast_math=not args.exact)
+        T, rows, layout = best_batch_config(shape, fast_math=not args.exact)
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=rows, fast_math=not args.exact,
+                        layout=layout)
     plan = BatchPlan([(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs], cfg)
     for i, sp in enumerate(specs):
         I0, I1, _, _ = synthetic.generate(sp)
@@ -255,7 +260,8 @@ def measure_batched(args, rank, flush, peak):
     return {
         "workload": f"hs_batched_{len(specs)}pairs_mixed", "pairs": len(specs),
         "mpix": round(sum(sp.H * sp.W for sp in specs) / 1e6, 3), "pix_iters": px_it,
-        "sweeps_per_pass": T, "rows_per_tile": rows, "autotuned": args.batch_sweeps_per_pass == 0,
+        "sweeps_per_pass": T, "rows_per_tile": rows, "columns_per_lane": 2 * layout if layout else "auto",
+        "autotuned": args.batch_sweeps_per_pass == 0,
         "launch": "one persistent kernel per batch, CUDA graph replay",
         "value": px_it * args.steps / t_b / 1e6, "unit": UNIT,
         "ms_per_step": t_b / args.steps * 1e3,
@@ -612,10 +618,13 @@ def main():
     stream = torch.cuda.current_stream()
 
     if args.sweeps_per_pass > 0:
-        T, seg = args.sweeps_per_pass, 0
+        T, seg, layout = args.sweeps_per_pass, 0, args.layout
     else:
-        T, seg = autotune.best_sweep_config(H, W, ld, fast_math=not args.exact)
-    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=not args.exact)
+        T, seg, layout = autotune.best_sweep_config(H, W, ld, fast_math=not args.exact)
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=not args.exact,
+                        layout=layout)
+    # the layout the library runs (hs_config.layout 0 chooses by image size)
+    wide = (not args.exact) and (layout == 2 or (layout == 0 and H * W >= 2_000_000))
     passes = (iters + T - 1) // T
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
@@ -694,13 +703,15 @@ def main():
         "data": "synthetic (seeded blurred noise + sinusoidal flow; see hindemith_b200/synthetic.py)",
         "config": {"workload": workload, "H": H, "W": W, "iters": iters,
                    "alpha": alpha, "sweeps_per_pass": T, "rows_per_segment": seg,
+                   "columns_per_lane": 4 if wide else 2,
                    "fast_math": not args.exact, "pairs_per_rank": 1,
                    "l2": "flushed between steps (256 MiB write); the 41 MB working set of one "
                          "pair is L2-resident within a step",
                    "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": f"hs_stream_kernel<{T},{'false' if args.exact else 'true'}>",
+                     "kernel": (f"hs_stream_w_kernel<{T}>" if wide else
+                                f"hs_stream_kernel<{T},{'false' if args.exact else 'true'}>"),
                      "peak_source": peak_kind,
                      "bytes_per_launch": BYTES_PER_PX_PASS * H * W,
                      "avg_launch_us": launch_s * 1e6},

@@ -47,7 +47,7 @@ class hs_config(ctypes.Structure):
         ("fast_math", ctypes.c_int),
         ("avg_edge", ctypes.c_float),
         ("avg_corner", ctypes.c_float),
-        ("reserved", ctypes.c_int * 3),
+        ("layout", ctypes.c_int), ("reserved", ctypes.c_int * 2),
     ]
 
 
@@ -182,8 +182,9 @@ def check(status: int, func: str) -> None:
 
 
 def make_config(sweeps_per_pass=0, rows_per_segment=0, fast_math=False, avg_edge=0.0,
-                avg_corner=0.0) -> hs_config:
+                avg_corner=0.0, layout=0) -> hs_config:
     c = hs_config()
+    c.layout = int(layout)
     c.sweeps_per_pass = int(sweeps_per_pass)
     c.rows_per_segment = int(rows_per_segment)
     c.fast_math = 1 if fast_math else 0

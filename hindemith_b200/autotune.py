@@ -58,13 +58,13 @@ def _save_file():
             pass
 
 
-def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=3):
+def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=3, layout=0):
     import torch
 
     from . import _lib as L
     from . import device as D
 
-    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=fast_math)
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=fast_math, layout=layout)
     D.hs_sweeps(Ix, Iy, It, 1.0, T, u, v, cfg)  # warm-up, first-launch attributes
     best = float("inf")
     for _ in range(reps):
@@ -79,19 +79,20 @@ def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=3):
 
 
 def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
-                      candidates=T_CANDIDATES) -> Tuple[int, int]:
-    """(sweeps_per_pass, rows_per_segment) fastest on the current device for HxW."""
+                      candidates=T_CANDIDATES) -> Tuple[int, int, int]:
+    """(sweeps_per_pass, rows_per_segment, layout) fastest on the current device for HxW;
+    both layouts (2 and 4 columns per lane) compete in the fast form."""
     import torch
 
     from . import device as D
 
     dev_name = torch.cuda.get_device_name()
-    key = _key(dev_name, H, W, ld, fast_math)
+    key = _key(dev_name, H, W, ld, fast_math) + "|layout"
     with _lock:
         if not _cache:
             _load_file()
         if key in _cache:
-            return _cache[key]
+            return tuple(_cache[key])
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     planes = D.empty_planes(5, H, W)
@@ -100,18 +101,19 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
     Ix, Iy, It, u, v = planes
     sweeps = 120  # a multiple of every candidate T
     results = []
-    for T in candidates:
-        for seg in _seg_candidates(H, W, T):
-            ms = time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps)
-            results.append((ms, T, seg))
+    for layout in ((1, 2) if fast_math else (1,)):
+        for T in candidates:
+            for seg in _seg_candidates(H, W, T):
+                ms = time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, layout=layout)
+                results.append((ms, T, seg, layout))
     results.sort()
-    best = (results[0][1], results[0][2])
+    best = tuple(results[0][1:])
     log = os.environ.get("HS_AUTOTUNE_LOG")
     if log:
         try:
             with open(log, "a") as f:
                 f.write(json.dumps({"key": key, "sweeps": sweeps,
-                                    "ms": [[round(ms, 5), T, seg] for ms, T, seg in results]}) + "\n")
+                                    "ms": [[round(r[0], 5), *r[1:]] for r in results]}) + "\n")
         except OSError:
             pass
     with _lock:
@@ -125,7 +127,9 @@ def clear():
         _cache.clear()
 
 
-BATCH_CANDIDATES = ((3, 96), (4, 64), (4, 96), (5, 96), (5, 128), (6, 128))
+# (T, rows per tile, layout): 1 = 2 columns per lane, 2 = 4 (fast form only)
+BATCH_CANDIDATES = ((3, 96, 1), (4, 64, 1), (4, 96, 1), (5, 96, 1), (5, 128, 1), (6, 128, 1),
+                    (4, 64, 2), (4, 96, 2), (5, 96, 2), (5, 128, 2), (6, 128, 2))
 
 
 def _log(entry):
@@ -139,8 +143,8 @@ def _log(entry):
 
 
 def best_batch_config(specs, fast_math: bool = True, candidates=BATCH_CANDIDATES,
-                      reps: int = 3) -> Tuple[int, int]:
-    """(sweeps_per_pass, rows_per_segment) fastest for the persistent batched launch of
+                      reps: int = 3) -> Tuple[int, int, int]:
+    """(sweeps_per_pass, rows_per_segment, layout) fastest for the persistent batched launch of
     `specs` = [(H, W, alpha, iters)] on the current device (timed as CUDA-graph replays
     of the batch itself over seeded random planes)."""
     import hashlib
@@ -152,18 +156,20 @@ def best_batch_config(specs, fast_math: bool = True, candidates=BATCH_CANDIDATES
 
     sig = hashlib.sha1(repr(sorted((int(H), int(W), float(a), int(n)) for H, W, a, n in specs))
                        .encode()).hexdigest()[:16]
-    key = f"{torch.cuda.get_device_name()}|batch{len(specs)}:{sig}|{'fast' if fast_math else 'exact'}"
+    key = f"{torch.cuda.get_device_name()}|batch{len(specs)}:{sig}|{'fast' if fast_math else 'exact'}|layout"
     with _lock:
         if not _cache:
             _load_file()
         if key in _cache:
-            return _cache[key]
+            return tuple(_cache[key])
     g = torch.Generator(device="cuda")
     g.manual_seed(0)
     results = []
-    for T, rows in candidates:
+    for T, rows, layout in candidates:
+        if layout == 2 and not fast_math:
+            continue
         plan = BatchPlan(specs, L.make_config(sweeps_per_pass=T, rows_per_segment=rows,
-                                              fast_math=fast_math))
+                                              fast_math=fast_math, layout=layout))
         for a, b in zip(plan.I0, plan.I1):
             a.copy_(torch.rand(a.shape, device="cuda", generator=g))
             b.copy_(torch.rand(b.shape, device="cuda", generator=g))
@@ -180,11 +186,11 @@ def best_batch_config(specs, fast_math: bool = True, candidates=BATCH_CANDIDATES
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))
         plan.check()
-        results.append((best, T, rows))
+        results.append((best, T, rows, layout))
         del plan
     results.sort()
-    best = (results[0][1], results[0][2])
-    _log({"key": key, "ms": [[round(ms, 4), T, r] for ms, T, r in results]})
+    best = tuple(results[0][1:])
+    _log({"key": key, "ms": [[round(r[0], 4), *r[1:]] for r in results]})
     with _lock:
         _cache[key] = best
         _save_file()

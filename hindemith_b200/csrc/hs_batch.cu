@@ -26,7 +26,7 @@
 #include <numeric>
 #include <vector>
 
-#include "hs_stream.cuh"
+#include "hs_stream4.cuh"
 
 namespace hs {
 
@@ -130,13 +130,21 @@ __device__ __forceinline__ void decode(const BatchParams &bp, int g, int &pass, 
     local = t - bp.item_prefix[lo];
 }
 
-template <int T, bool FAST>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3 : 2)))
+template <int T, bool WIDE>
+constexpr int batch_min_blocks() { return WIDE ? (T <= 4 ? 3 : 2) : (T <= 4 ? 4 : (T <= 6 ? 3 : 2)); }
+template <int T, bool WIDE>
+constexpr int batch_warp_floats() { return WIDE ? GeoW<T>::warp_floats : Geo<T>::warp_floats; }
+template <int T, bool WIDE>
+constexpr int batch_smem() { return WIDE ? GeoW<T>::smem_bytes : Geo<T>::smem_bytes; }
+
+// WIDE: the fast form in the 4-columns-per-lane layout (128-column tiles).
+template <int T, bool FAST, bool WIDE>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (batch_min_blocks<T, WIDE>()))
     hs_batch_kernel(const __grid_constant__ BatchParams bp) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    float *wbase = reinterpret_cast<float *>(smem4) + warp * Geo<T>::warp_floats;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * batch_warp_floats<T, WIDE>();
 
     griddep_launch_dependents();
     griddep_wait();
@@ -184,9 +192,15 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
         sp.seg_rows = P.seg_rows;
         sp.nstrips = P.nstrips;
         sp.nitems = P.items;
-        Item it;
-        init_item<T>(it, sp, strip, seg, lane, wbase);
-        run_item<T, FAST>(sp, it);
+        if constexpr (WIDE) {
+            ItemW it;
+            init_item_w<T>(it, sp, strip, seg, lane, wbase);
+            run_item_w<T>(sp, it);
+        } else {
+            Item it;
+            init_item<T>(it, sp, strip, seg, lane, wbase);
+            run_item<T, FAST>(sp, it);
+        }
 
         // every lane makes its own stores visible GPU-wide before the warp publishes
         __threadfence();
@@ -208,6 +222,13 @@ static int batch_seg_rows(int H, int T, int cfg_rows) {
     return std::min(H, std::max(96, T));
 }
 
+// The whole batch runs one layout: the wide one when the pairs average a large image.
+static bool batch_wide(const ResolvedConfig &rc, const hs_pair_desc *pairs, int n) {
+    long px = 0;
+    for (int i = 0; i < n; ++i) px += (long)pairs[i].H * pairs[i].W;
+    return use_wide(rc, px / n);
+}
+
 static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *cfg,
                             ResolvedConfig &rc, std::vector<PairPlan> &plan, size_t &total) {
     hs_status st = resolve_config(cfg, &rc);
@@ -215,6 +236,7 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
     if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
     if (n < 1 || n > kMaxBatch) HS_FAIL(HS_ERR_INVALID_ARG, "n=%d outside 1..%d", n, kMaxBatch);
     const int T = rc.T;
+    const int sc = batch_wide(rc, pairs, n) ? strip_cols_wide(T) : strip_cols_for(T);
     plan.clear();
     size_t off = kHeaderBytes;
     for (int i = 0; i < n; ++i) {
@@ -232,7 +254,7 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
         p.rem = d.iters % T;
         const int total_passes = p.passes + (p.rem ? 1 : 0);
         p.start = total_passes & 1;  // the last pass writes buffer 0, the caller's u, v
-        p.nstrips = (d.W + strip_cols_for(T) - 1) / strip_cols_for(T);
+        p.nstrips = (d.W + sc - 1) / sc;
         p.seg_rows = batch_seg_rows(d.H, T, rc.seg_rows);
         p.nseg = (d.H + p.seg_rows - 1) / p.seg_rows;
         p.items = p.nstrips * p.nseg;
@@ -248,9 +270,10 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
     return HS_OK;
 }
 
-template <int T, bool FAST>
+template <int T, bool FAST, bool WIDE>
 static hs_status launch_batch(const BatchParams &bp, cudaStream_t stream) {
-    auto fn = hs_batch_kernel<T, FAST>;
+    auto fn = hs_batch_kernel<T, FAST, WIDE>;
+    constexpr int smem = batch_smem<T, WIDE>();
     static std::mutex mu;
     static int blocks_per_sm[64] = {};
     int dev = 0;
@@ -259,11 +282,9 @@ static hs_status launch_batch(const BatchParams &bp, cudaStream_t stream) {
     {
         std::lock_guard<std::mutex> lock(mu);
         if (dev < 64 && blocks_per_sm[dev] == 0) {
-            HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               Geo<T>::smem_bytes));
+            HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
             int b = 0;
-            HS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kWarpsPerBlock * 32,
-                                                                        Geo<T>::smem_bytes));
+            HS_CUDA_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, fn, kWarpsPerBlock * 32, smem));
             blocks_per_sm[dev] = std::max(b, 1);
         }
         bps = dev < 64 ? blocks_per_sm[dev] : 1;
@@ -273,7 +294,7 @@ static hs_status launch_batch(const BatchParams &bp, cudaStream_t stream) {
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)std::max(1L, std::min(want, need)));
     cfg.blockDim = dim3(kWarpsPerBlock * 32);
-    cfg.dynamicSmemBytes = Geo<T>::smem_bytes;
+    cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -284,9 +305,11 @@ static hs_status launch_batch(const BatchParams &bp, cudaStream_t stream) {
     return HS_OK;
 }
 
-static hs_status launch_batch_any(int T, bool fast, const BatchParams &bp, cudaStream_t s) {
-#define HS_CASE(TT)                                                                 \
-    case TT: return fast ? launch_batch<TT, true>(bp, s) : launch_batch<TT, false>(bp, s);
+static hs_status launch_batch_any(int T, bool fast, bool wide, const BatchParams &bp, cudaStream_t s) {
+#define HS_CASE(TT)                                                                  \
+    case TT:                                                                         \
+        return wide ? launch_batch<TT, true, true>(bp, s)                            \
+                    : (fast ? launch_batch<TT, true, false>(bp, s) : launch_batch<TT, false, false>(bp, s));
     switch (T) {
         HS_CASE(1) HS_CASE(2) HS_CASE(3) HS_CASE(4) HS_CASE(5) HS_CASE(6) HS_CASE(7) HS_CASE(8)
     }
@@ -429,7 +452,7 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
     bp.ngroups = ng;
     bp.total_items = (int)total_items;
     if (total_items > 0)
-        if ((st = launch_batch_any(rc.T, rc.fast, bp, s)) != HS_OK) return st;
+        if ((st = launch_batch_any(rc.T, rc.fast, batch_wide(rc, pairs, n), bp, s)) != HS_OK) return st;
 
     // the short last pass of pairs whose sweep count is not a multiple of T
     for (int i = 0; i < n; ++i) {

@@ -356,8 +356,12 @@ struct ResolvedConfig {
     int T;
     int seg_rows;  // 0 = derive per pass
     bool fast;
+    int layout;    // hs_config.layout: 0 automatic, 1 two columns per lane, 2 four
     float we, wc;
 };
+// whether the sweeps of an H x W image (or a batch averaging that size) run in the
+// 4-columns-per-lane layout
+bool use_wide(const ResolvedConfig &rc, long pixels);
 hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out);
 int strip_cols_for(int T);
 int default_seg_rows(int H, int nstrips, int T);

@@ -94,6 +94,11 @@ def test_sweep_argument_checks():
     bad.reserved[1] = 3
     st = lib.hs_forward(P, P, H, W, ld, 1.0, 5, P, P, P, 10 ** 6, ctypes.byref(bad), None)
     assert st == L.HS_ERR_INVALID_ARG
+    # layout outside 0..2, and the 4-column layout without the fast form
+    for bad in (L.make_config(layout=3), L.make_config(layout=2, fast_math=False)):
+        st = lib.hs_forward(P, P, H, W, ld, 1.0, 5, P, P, P, 10 ** 6, ctypes.byref(bad), None)
+        assert st == L.HS_ERR_INVALID_ARG
+        assert "layout" in L.lib().hs_last_error().decode()
     st = lib.hs_forward(P, P, H, W, ld, 1.0, 5, P, P, P, 10, ctypes.byref(cfg), None)
     assert st == L.HS_ERR_WORKSPACE
 

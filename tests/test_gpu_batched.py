@@ -102,3 +102,18 @@ def test_forward_batched_eager_api(cuda):
         ru, rv = O.c_hs_forward(a, b, np.float32(s[2]), s[3])
         assert_bitexact(u.cpu().numpy(), ru, "u")
         assert_bitexact(v.cpu().numpy(), rv, "v")
+
+
+@pytest.mark.parametrize("T", [3, 4, 6, 8])
+def test_batched_wide_layout_equals_per_pair(cuda, T):
+    """The persistent launch in the 4-columns-per-lane layout (128-column tiles) equals the
+    per-pair forward in the 2-column layout, bit for bit."""
+    inputs = make_inputs(MIXED)
+    plan = run_plan(MIXED, L.make_config(sweeps_per_pass=T, fast_math=True, layout=2), inputs)
+    narrow = L.make_config(sweeps_per_pass=T, fast_math=True, layout=1)
+    for i, ((H, W, alpha, iters), (I0, I1)) in enumerate(zip(MIXED, inputs)):
+        u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()),
+                            D.as_plane(torch.from_numpy(I1).cuda()), alpha, iters, narrow)
+        torch.cuda.synchronize()
+        assert_bitexact(plan.u[i].cpu().numpy(), u.cpu().numpy(), f"u pair {i}")
+        assert_bitexact(plan.v[i].cpu().numpy(), v.cpu().numpy(), f"v pair {i}")

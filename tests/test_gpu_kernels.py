@@ -172,3 +172,37 @@ def test_misaligned_plane_is_rejected(cuda):
     lib = L.lib()
     st = lib.hs_array2d_copy(D.ptr(shifted), D.ptr(base), 8, 8, 8, None)
     assert st == L.HS_ERR_ALIGNMENT
+
+
+WIDE_SHAPES = [(1, 1), (1, 5), (67, 1), (1, 67), (3, 5), (2, 200), (130, 257), (257, 130), (64, 128)]
+
+
+@pytest.mark.parametrize("shape", WIDE_SHAPES)
+@pytest.mark.parametrize("T", [1, 3, 4, 5, 8])
+def test_wide_layout_equals_narrow(cuda, shape, T):
+    """The fast form's 4-columns-per-lane layout computes every cell with the same
+    arithmetic as the 2-column one: identical results, bit for bit, at every shape, depth
+    and segmentation."""
+    H, W = shape
+    rng = np.random.default_rng(H * 1000 + W + T)
+    Ix, Iy, It, u0, v0 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(5))
+    ref = run_sweeps(Ix, Iy, It, 0.8, 23, u0, v0, sweeps_per_pass=T, fast_math=True, layout=1)
+    for seg in (0, 3):
+        got = run_sweeps(Ix, Iy, It, 0.8, 23, u0, v0, sweeps_per_pass=T, fast_math=True,
+                         layout=2, rows_per_segment=seg)
+        assert_bitexact(got[0], ref[0], "u")
+        assert_bitexact(got[1], ref[1], "v")
+
+
+def test_wide_layout_full_size(cuda):
+    """1920x1080, 60 sweeps: the automatic layout (wide at this size) equals the narrow one
+    and stays within 1e-4 of FP64."""
+    I0, I1, _, _ = synthetic.generate(synthetic.plain_1080p())
+    Ix, Iy, It = O.c_hs_derivs(I0, I1)
+    z = np.zeros_like(I0)
+    ref = run_sweeps(Ix, Iy, It, 1.0, 60, z, z, sweeps_per_pass=5, fast_math=True, layout=1)
+    got = run_sweeps(Ix, Iy, It, 1.0, 60, z, z, sweeps_per_pass=5, fast_math=True, layout=0)
+    assert_bitexact(got[0], ref[0], "u")
+    assert_bitexact(got[1], ref[1], "v")
+    u64, v64 = O.c_hs_sweeps(Ix, Iy, It, 1.0, 60, z, z, np.float64)
+    assert np.abs(got[0] - u64).max() < FAST_TOL and np.abs(got[1] - v64).max() < FAST_TOL
