@@ -155,6 +155,42 @@ def cpu_baseline(I0, I1, alpha, sweeps):
             "sample": f"{W}x{H}, {sweeps} sweeps of the 500-sweep workload, derivatives included"}
 
 
+def cpu_baselines_other():
+    """The CPU restatements of the other operators, each on a bounded sample, on all host
+    cores (the matrix powers, the preconditioners, LK and the DIA product are OpenMP loops;
+    the Brox matrix fill is serial), as rates comparable to the GPU legs."""
+    import numpy as np
+
+    from oracle import hs_oracle as O
+
+    rng = np.random.default_rng(1)
+
+    def timed(fn, *a):
+        fn(*a)  # warm
+        t0 = time.perf_counter()
+        fn(*a)
+        return time.perf_counter() - t0
+
+    out = {"cores": O.c_num_threads(), "kind": "port"}
+    H = W = 1024
+    Ix, Iy, r0, r1, d0, d1, od = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(7))
+    t = timed(O.c_hs_matrix_powers, 0.5, Ix, Iy, r0, r1, 9)
+    out["matrix_powers"] = {"sample": "1024x1024, 9 steps", "ms_per_2048sq_call": t * 4e3}
+    t = timed(O.c_apply_hs_precond, 0.25, d0, d1, od, r0, r1)
+    out["hs_preconditioner"] = {"sample": "1024x1024", "ms_per_2048sq_call": t * 4e3}
+    Hl, Wl = 270, 480
+    t = timed(O.c_lk_least_squares, Ix[:Hl, :Wl], Iy[:Hl, :Wl], r0[:Hl, :Wl], 5)
+    out["lk"] = {"sample": "480x270, radius 5", "ms_per_1080p_call": t * 16e3}
+    psi = np.abs(d0) + 0.1
+    t = timed(O.c_set_brox_matrix, psi, 0.5, np.zeros((5, H, W), np.float32))
+    data = O.c_set_brox_matrix(psi, 0.5, np.zeros((5, H, W), np.float32))
+    t2 = timed(O.c_spmv_dia2d, data, O.BROX_OFFX, O.BROX_OFFY, r0)
+    t3 = timed(O.c_apply_brox_precond, data[2], d0, d1, od, r0, r1)
+    out["brox"] = {"sample": "1024x1024", "set_matrix_ms_per_2048sq": t * 4e3,
+                   "spmv_ms_per_2048sq": t2 * 4e3, "preconditioner_ms_per_2048sq": t3 * 4e3}
+    return out
+
+
 def run_reference(args, rank, world):
     """--impl reference: the host-core restatement of the reference's kernels."""
     from hindemith_b200 import synthetic
@@ -735,6 +771,8 @@ def main():
         line["pyramid"] = measure_pyramid(args, rank, flush)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(I0h, I1h, alpha, args.cpu_sample_sweeps)
+        if "cg" in line:
+            line["cpu_baseline_other_operators"] = cpu_baselines_other()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
