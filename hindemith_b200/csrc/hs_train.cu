@@ -136,6 +136,9 @@ struct AdjGeo {
 
 // M of one sweep at one column: lambda (lu, lv) -> z, adding this sweep's gradient terms to
 // acc (aIx, aIy, aIt, aA2).  C = (Ix, Iy, It, 1/d); (xu, xv) = x_{k+1}.
+// With g = Ix lu + Iy lv, lr = -g/d, t = (Ix xu + Iy xv + It)/alpha^2 and z = lambda + lr (Ix, Iy):
+//   dIx += -lu t + lr ubar + 2 Ix (g t / d) = lr xu - t zu   (ubar = xu + Ix t, g t / d = -lr t)
+//   dIy += lr xv - t zv,   dIt += lr,   dalpha^2 += -lr t
 __device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, float xu, float xv,
                                           float inv_a2, float &zu, float &zv, float4 &acc) {
     const float g = fmaf(C.x, lu, C.y * lv);
@@ -143,12 +146,10 @@ __device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, f
     zu = fmaf(lr, C.x, lu);
     zv = fmaf(lr, C.y, lv);
     const float t = fmaf(C.x, xu, fmaf(C.y, xv, C.z)) * inv_a2;
-    const float ub = fmaf(C.x, t, xu), vb = fmaf(C.y, t, xv);
-    const float ld = g * t * C.w;
-    acc.x = fmaf(-lu, t, fmaf(lr, ub, fmaf(2.f * C.x, ld, acc.x)));
-    acc.y = fmaf(-lv, t, fmaf(lr, vb, fmaf(2.f * C.y, ld, acc.y)));
+    acc.x = fmaf(-t, zu, fmaf(lr, xu, acc.x));
+    acc.y = fmaf(-t, zv, fmaf(lr, xv, acc.y));
     acc.z += lr;
-    acc.w += ld;
+    acc.w = fmaf(-lr, t, acc.w);
 }
 
 // Global loads one step ahead: the state rows every stage uses at step k.
