@@ -625,6 +625,7 @@ def main():
     from hindemith_b200 import device as D
     from hindemith_b200 import synthetic
     from hindemith_b200 import autotune
+    from hindemith_b200.replicas import job_rate, max_over_ranks, rank_seed
 
     if not torch.cuda.is_available():
         raise SystemExit("bench.py: no CUDA device (libhsflow has no CPU path)")
@@ -638,7 +639,7 @@ def main():
     warmup = max(args.warmup, 3)
 
     spec = synthetic.plain_1080p()
-    spec.seed = 1000 + rank
+    spec.seed = rank_seed(spec.seed, rank)
     workload = "hs_plain_1920x1080_500sweeps"
     if args.shape:
         spec.H, spec.W = (int(x) for x in args.shape.lower().split("x"))
@@ -712,14 +713,11 @@ def main():
         t_e2e = e2e_pipelined(I0h, I1h, alpha, iters, cfg, args.steps, flush, dist)
     clocks = clk.summary()
 
-    times = torch.tensor([t_step, t_sweeps, t_e2e], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    t_step, t_sweeps, t_e2e = times.tolist()
+    t_step, t_sweeps, t_e2e = max_over_ranks([t_step, t_sweeps, t_e2e])
 
     px_iters = H * W * iters * args.steps * world
-    value = px_iters / t_step / 1e6
-    e2e_value = px_iters / t_e2e / 1e6
+    value = job_rate(H * W * iters * args.steps, world, t_step) / 1e6
+    e2e_value = job_rate(H * W * iters * args.steps, world, t_e2e) / 1e6
     peak, peak_kind = load_peaks()
     launch_s = t_sweeps / (args.steps * passes)
     achieved = BYTES_PER_PX_PASS * H * W / launch_s / 1e9
