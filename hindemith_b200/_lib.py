@@ -131,6 +131,7 @@ SIGNATURES = {
     "hs_backward_batched": (_i, [_tpp, _i, _i, _i, _vp, _sz, _cfgp, _vp]),
     "hs_matrix_powers": (_i, [_f, _vp, _vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _sz, _cfgp, _vp]),
     "hs_apply_hs_preconditioner": (_i, [_f, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp]),
+    "hs_selftest_bounded_wait": (_i, [_vp, _i, _vp]),
     "hs_lk_least_squares": (_i, [_vp, _vp, _vp, _i, _i, _i, _i, _vp, _vp, _vp]),
     "hs_set_brox_matrix": (_i, [_vp, _i, _i, _i, _f, _vp, _sz, _i, _vp, _vp]),
     "hs_spmv_dia2d": (_i, [_vp, _sz, _ip, _ip, _i, _vp, _i, _i, _i, _vp, _vp]),

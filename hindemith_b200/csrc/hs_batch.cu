@@ -87,6 +87,20 @@ __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Poll `flag` until it reaches `need`, with exponential nanosleep back-off; gives up (false)
+// after `max_polls` polls in all (`polls` carries the count across calls) or when
+// *abort_flag is raised.
+__device__ bool wait_flag_ge(const unsigned *flag, unsigned need, const unsigned *abort_flag,
+                             unsigned long long max_polls, unsigned long long &polls, unsigned &ns) {
+    while (ld_acquire(flag) < need) {
+        if (++polls > max_polls) return false;
+        if ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag) return false;
+        __nanosleep(ns);
+        ns = min(ns * 2, 256u);
+    }
+    return true;
+}
+
 // Lane 0: wait until tiles (seg+-1, strip+-1) of pair P have completed `need` passes.
 // Returns false if the wait gave up or another warp aborted.
 __device__ bool wait_neighbours(const BatchPair &P, int seg, int strip, unsigned need,
@@ -101,15 +115,24 @@ __device__ bool wait_neighbours(const BatchPair &P, int seg, int strip, unsigned
             const int s = strip + ds;
             if (s < 0 || s >= P.nstrips) continue;
             const unsigned *flag = P.progress + (size_t)g * P.nstrips + s;
-            while (ld_acquire(flag) < need) {
-                if (++polls > kWaitPolls) return false;
-                if ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag) return false;
-                __nanosleep(ns);
-                ns = min(ns * 2, 256u);
-            }
+            if (!wait_flag_ge(flag, need, abort_flag, kWaitPolls, polls, ns)) return false;
         }
     }
     return true;
+}
+
+// Self-test of the failure path: one thread waits, with the batched kernel's bounded wait,
+// on a flag that no code ever sets; the wait gives up and reports HS_ERR_TIMEOUT through
+// the status word, and the kernel returns (the context stays usable).
+__device__ unsigned g_never_set_flag = 0;
+__device__ unsigned g_selftest_abort = 0;
+
+__global__ void wait_selftest_kernel(int *status, unsigned long long max_polls) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long polls = 0;
+    unsigned ns = 32;
+    if (!wait_flag_ge(&g_never_set_flag, 1u, &g_selftest_abort, max_polls, polls, ns))
+        atomicCAS(status, 0, (int)HS_ERR_TIMEOUT);
 }
 
 // (pass, pair, local tile) of work item `g`.
@@ -482,6 +505,16 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
         pp.nitems = pp.nstrips * ((p.H + pp.seg_rows - 1) / pp.seg_rows);
         if ((st = launch_pass(p.rem, rc.fast, pp, s)) != HS_OK) return st;
     }
+    return HS_OK;
+}
+
+hs_status hs_selftest_bounded_wait(int *device_status, int max_polls, void *stream) {
+    clear_error();
+    if (!device_status) HS_FAIL(HS_ERR_INVALID_ARG, "device_status is NULL");
+    if (max_polls < 1 || (unsigned long long)max_polls > kWaitPolls)
+        HS_FAIL(HS_ERR_INVALID_ARG, "max_polls=%d outside 1..%llu", max_polls, kWaitPolls);
+    wait_selftest_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(device_status, (unsigned long long)max_polls);
+    HS_LAUNCH_CHECK("wait_selftest_kernel");
     return HS_OK;
 }
 

@@ -278,6 +278,13 @@ HS_API hs_status hs_apply_hs_preconditioner(float s2, const float *diag0, const 
                                             const float *x1, int H, int W, int ld, float *y0,
                                             float *y1, void *stream);
 
+/* Self-test of the failure path of the batched launch's bounded waits (no counterpart in
+ * the reference, whose runtime has no device-side waits): one thread waits with the same
+ * bounded wait on a flag that nothing sets, gives up after max_polls polls
+ * (1 .. 2^22, with a nanosleep back-off of at most 256 ns each) and writes HS_ERR_TIMEOUT to
+ * *device_status (a device int the caller zeroed).  The kernel then returns normally. */
+HS_API hs_status hs_selftest_bounded_wait(int *device_status, int max_polls, void *stream);
+
 /* ---- Lucas-Kanade and Brox on the same grid substrate -------------------------- */
 
 /* LKLeastSquares.cpp:44-79: for pixels at least `radius` from the left/top border and

@@ -198,3 +198,9 @@ def test_lk_brox_argument_checks():
     assert lib.hs_spmv_dia2d(P, 64, ox, ox, 17, P, 8, 8, 8, fake_ptr(256), None) == L.HS_ERR_INVALID_ARG
     assert lib.hs_spmv_dia2d(P, 64, ox, ox, 5, P, 8, 8, 8, P, None) == L.HS_ERR_INVALID_ARG  # x == y
     assert lib.hs_apply_brox_preconditioner(P, P, P, P, P, P, 8, 8, 8, P, fake_ptr(2), None) == L.HS_ERR_ALIGNMENT
+
+
+def test_selftest_wait_argument_checks():
+    lib = L.lib()
+    assert lib.hs_selftest_bounded_wait(None, 16, None) == L.HS_ERR_INVALID_ARG
+    assert lib.hs_selftest_bounded_wait(fake_ptr(), 0, None) == L.HS_ERR_INVALID_ARG

@@ -117,3 +117,26 @@ def test_batched_wide_layout_equals_per_pair(cuda, T):
         torch.cuda.synchronize()
         assert_bitexact(plan.u[i].cpu().numpy(), u.cpu().numpy(), f"u pair {i}")
         assert_bitexact(plan.v[i].cpu().numpy(), v.cpu().numpy(), f"v pair {i}")
+
+
+def test_bounded_wait_times_out_and_context_survives(cuda):
+    """A device-side wait on a flag that nothing sets gives up after its poll limit and
+    reports HS_ERR_TIMEOUT through the status word; the context stays usable."""
+    import ctypes
+    import time
+
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    t0 = time.perf_counter()
+    L.check(L.lib().hs_selftest_bounded_wait(ctypes.c_void_p(status.data_ptr()), 1 << 16,
+                                             D.stream_handle()), "hs_selftest_bounded_wait")
+    torch.cuda.synchronize()
+    assert int(status.item()) == L.HS_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 60
+    # the next launches run normally
+    inputs = make_inputs(MIXED[:3])
+    cfg = L.make_config(sweeps_per_pass=4)
+    plan = run_plan(MIXED[:3], cfg, inputs)
+    I0, I1 = inputs[2]
+    u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()), D.as_plane(torch.from_numpy(I1).cuda()),
+                        MIXED[2][2], MIXED[2][3], cfg)
+    assert_bitexact(plan.u[2].cpu().numpy(), u.cpu().numpy())
