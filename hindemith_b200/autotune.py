@@ -129,7 +129,7 @@ def clear():
 
 # (T, rows per tile, layout): 1 = 2 columns per lane, 2 = 4 (fast form only)
 BATCH_CANDIDATES = ((3, 96, 1), (4, 64, 1), (4, 96, 1), (5, 96, 1), (5, 128, 1), (6, 128, 1),
-                    (4, 64, 2), (4, 96, 2), (5, 96, 2), (5, 128, 2), (6, 128, 2))
+                    (6, 96, 1), (6, 128, 2))
 
 
 def _log(entry):
@@ -166,8 +166,10 @@ def best_batch_config(specs, fast_math: bool = True, candidates=BATCH_CANDIDATES
     g.manual_seed(0)
     results = []
     for T, rows, layout in candidates:
-        if layout == 2 and not fast_math:
-            continue
+        if layout != 1 and not fast_math:
+            if (T, rows, 1) in candidates:
+                continue
+            layout = 1
         plan = BatchPlan(specs, L.make_config(sweeps_per_pass=T, rows_per_segment=rows,
                                               fast_math=fast_math, layout=layout))
         for a, b in zip(plan.I0, plan.I1):

@@ -31,7 +31,7 @@
 namespace hs {
 
 constexpr int kMaxBatch = HS_MAX_BATCH;
-constexpr int kHeaderBytes = 256;                 // queue counter, status, abort flag
+constexpr int kHeaderBytes = 256;  // queue counters (2-column and 4-column launch), status, abort flag
 constexpr unsigned long long kWaitPolls = 1ull << 22;  // bounded wait (seconds, at most)
 
 struct BatchPair {
@@ -237,19 +237,13 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (batch_min_blocks<T, WIDE
 struct PairPlan {
     int idx;  // position in the caller's array
     int H, W, ld, iters, passes, rem, start, nstrips, seg_rows, nseg, items;
+    bool wide;
     size_t off_planes, off_progress;
 };
 
 static int batch_seg_rows(int H, int T, int cfg_rows) {
     if (cfg_rows > 0) return std::max(std::min(cfg_rows, H), std::min(H, T));
     return std::min(H, std::max(96, T));
-}
-
-// The whole batch runs one layout: the wide one when the pairs average a large image.
-static bool batch_wide(const ResolvedConfig &rc, const hs_pair_desc *pairs, int n) {
-    long px = 0;
-    for (int i = 0; i < n; ++i) px += (long)pairs[i].H * pairs[i].W;
-    return use_wide(rc, px / n);
 }
 
 static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *cfg,
@@ -259,7 +253,6 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
     if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
     if (n < 1 || n > kMaxBatch) HS_FAIL(HS_ERR_INVALID_ARG, "n=%d outside 1..%d", n, kMaxBatch);
     const int T = rc.T;
-    const int sc = batch_wide(rc, pairs, n) ? strip_cols_wide(T) : strip_cols_for(T);
     plan.clear();
     size_t off = kHeaderBytes;
     for (int i = 0; i < n; ++i) {
@@ -277,6 +270,12 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
         p.rem = d.iters % T;
         const int total_passes = p.passes + (p.rem ? 1 : 0);
         p.start = total_passes & 1;  // the last pass writes buffer 0, the caller's u, v
+        // 4 columns per lane only when asked for (hs_config.layout = 2): in a persistent
+        // launch a tile's latency bounds the chain of dependent passes, and the wider tiles
+        // take twice as long (measured: the mixed 64-pair batch at T = 6 runs 37 ms with 2
+        // columns per lane, 61 ms with 4, 101 ms with each pair in its size's layout)
+        p.wide = rc.fast && rc.layout == 2;
+        const int sc = p.wide ? strip_cols_wide(T) : strip_cols_for(T);
         p.nstrips = (d.W + sc - 1) / sc;
         p.seg_rows = batch_seg_rows(d.H, T, rc.seg_rows);
         p.nseg = (d.H + p.seg_rows - 1) / p.seg_rows;
@@ -379,7 +378,6 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
     }
     cudaStream_t s = (cudaStream_t)stream;
     char *ws = reinterpret_cast<char *>(workspace);
-    unsigned *queue = reinterpret_cast<unsigned *>(ws);
     int *status = device_status ? device_status : reinterpret_cast<int *>(ws + 4);
     unsigned *abort_flag = reinterpret_cast<unsigned *>(ws + 8);
 
@@ -438,44 +436,50 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
         HS_LAUNCH_CHECK("batch_derivs_kernel");
     }
 
-    // persistent kernel over every full pass of every pair
-    std::vector<int> order(n);
-    std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int a, int b) { return bpairs[a].passes > bpairs[b].passes; });
-    BatchParams bp;
-    memset(&bp, 0, sizeof(bp));
-    bp.npairs = n;
-    bp.we = rc.we;
-    bp.wc = rc.wc;
-    bp.queue = queue;
-    bp.status = status;
-    bp.abort_flag = abort_flag;
-    bp.item_prefix[0] = 0;
-    for (int r = 0; r < n; ++r) {
-        bp.pair[r] = bpairs[order[r]];
-        bp.item_prefix[r + 1] = bp.item_prefix[r] + bp.pair[r].items;
-    }
-    // pass groups: runs of passes with the same number of active (sorted) pairs
-    long total_items = 0;
-    int ng = 0, p0 = 0;
-    for (int r = n; r >= 1; --r) {
-        const int p1 = bp.pair[r - 1].passes;  // the first r pairs are active for p < p1
-        if (p1 > p0) {
-            bp.g_p0[ng] = p0;
-            bp.g_p1[ng] = p1;
-            bp.g_active[ng] = r;
-            bp.g_first[ng] = (int)total_items;
-            total_items += (long)(p1 - p0) * bp.item_prefix[r];
-            ++ng;
-            p0 = p1;
+    // persistent kernels over every full pass of every pair: one launch per layout
+    for (int lay = 1; lay >= 0; --lay) {
+        const bool wide = lay == 1;
+        std::vector<int> order;
+        for (int i = 0; i < n; ++i)
+            if (plan[i].wide == wide) order.push_back(i);
+        if (order.empty()) continue;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return bpairs[a].passes > bpairs[b].passes; });
+        const int m = (int)order.size();
+        BatchParams bp;
+        memset(&bp, 0, sizeof(bp));
+        bp.npairs = m;
+        bp.we = rc.we;
+        bp.wc = rc.wc;
+        bp.queue = reinterpret_cast<unsigned *>(ws + (wide ? 12 : 0));
+        bp.status = status;
+        bp.abort_flag = abort_flag;
+        bp.item_prefix[0] = 0;
+        for (int r = 0; r < m; ++r) {
+            bp.pair[r] = bpairs[order[r]];
+            bp.item_prefix[r + 1] = bp.item_prefix[r] + bp.pair[r].items;
         }
+        // pass groups: runs of passes with the same number of active (sorted) pairs
+        long total_items = 0;
+        int ng = 0, p0 = 0;
+        for (int r = m; r >= 1; --r) {
+            const int p1 = bp.pair[r - 1].passes;  // the first r pairs are active for p < p1
+            if (p1 > p0) {
+                bp.g_p0[ng] = p0;
+                bp.g_p1[ng] = p1;
+                bp.g_active[ng] = r;
+                bp.g_first[ng] = (int)total_items;
+                total_items += (long)(p1 - p0) * bp.item_prefix[r];
+                ++ng;
+                p0 = p1;
+            }
+        }
+        if (total_items > 0x7fffffffL) HS_FAIL(HS_ERR_UNSUPPORTED, "batch has too many work items");
+        bp.ngroups = ng;
+        bp.total_items = (int)total_items;
+        if (total_items > 0)
+            if ((st = launch_batch_any(rc.T, rc.fast, wide, bp, s)) != HS_OK) return st;
     }
-    if (total_items > 0x7fffffffL) HS_FAIL(HS_ERR_UNSUPPORTED, "batch has too many work items");
-    bp.ngroups = ng;
-    bp.total_items = (int)total_items;
-    if (total_items > 0)
-        if ((st = launch_batch_any(rc.T, rc.fast, batch_wide(rc, pairs, n), bp, s)) != HS_OK) return st;
 
     // the short last pass of pairs whose sweep count is not a multiple of T
     for (int i = 0; i < n; ++i) {

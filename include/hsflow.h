@@ -62,9 +62,9 @@ typedef struct hs_config {
                              multiply-adds and a per-pixel reciprocal, within 1e-4 */
     float avg_edge;       /* weight of the 4 edge taps of the 3x3 average; 0 = 1/6 */
     float avg_corner;     /* weight of the 4 corner taps; 0 = 1/12 (both 0 = the HS stencil) */
-    int layout;           /* columns per lane of the sweep kernels: 0 = chosen by image size,
-                             1 = 2 (64-column strips), 2 = 4 (128-column strips; fast_math only).
-                             Results do not depend on it. */
+    int layout;           /* columns per lane of the sweep kernels: 0 = chosen by image size
+                             (the batched launch keeps 2), 1 = 2 (64-column strips), 2 = 4
+                             (128-column strips; fast_math only).  Results do not depend on it. */
     int reserved[2];      /* must be zero */
 } hs_config;
 

@@ -140,3 +140,20 @@ def test_bounded_wait_times_out_and_context_survives(cuda):
     u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()), D.as_plane(torch.from_numpy(I1).cuda()),
                         MIXED[2][2], MIXED[2][3], cfg)
     assert_bitexact(plan.u[2].cpu().numpy(), u.cpu().numpy())
+
+
+def test_batched_large_pair_auto_layout_equals_per_pair(cuda):
+    """A batch holding a pair above the size where the per-pass kernels switch to 4 columns
+    per lane: the batch (2 columns per lane unless asked otherwise) equals each pair's
+    forward, which runs in the 4-column layout."""
+    specs = [(1100, 1900, 1.1, 14), (65, 127, 1.7, 40), (1, 1, 1.0, 3), (240, 320, 0.9, 21)]
+    inputs = make_inputs(specs, 4000)
+    cfg = L.make_config(sweeps_per_pass=4, fast_math=True)
+    plan = run_plan(specs, cfg, inputs)
+    auto = L.make_config(sweeps_per_pass=4, fast_math=True, layout=0)
+    for i, ((H, W, alpha, iters), (I0, I1)) in enumerate(zip(specs, inputs)):
+        u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()),
+                            D.as_plane(torch.from_numpy(I1).cuda()), alpha, iters, auto)
+        torch.cuda.synchronize()
+        assert_bitexact(plan.u[i].cpu().numpy(), u.cpu().numpy(), f"u pair {i}")
+        assert_bitexact(plan.v[i].cpu().numpy(), v.cpu().numpy(), f"v pair {i}")
