@@ -724,6 +724,17 @@ def main():
 
         us.zero_(), vs.zero_()
         t_sweeps = timed(sweeps_only, args.steps, 2, "timed_sweeps")
+        # the same step in the exact form (the drop-in's default: the reference program's
+        # FP32 operations one rounding at a time, 2 columns per lane, its own tuned depth)
+        t_exact = None
+        if not args.exact and not args.shape:
+            Te, sege, _ = autotune.best_sweep_config(H, W, ld, fast_math=False)
+            cfg_e = L.make_config(sweeps_per_pass=Te, rows_per_segment=sege)
+
+            def exact_step():
+                D.hs_forward(I0, I1, alpha, iters, cfg_e, out=(u, v))
+
+            t_exact = timed(exact_step, max(1, args.steps // 2), 2, "timed_exact")
         # end to end through the public API: every step copies its pair in from pinned
         # host memory and its flow out to pinned host memory; the copies of one step overlap
         # the sweeps of the previous one (a copy stream, double-buffered device planes), as
@@ -733,6 +744,8 @@ def main():
     clocks = clk.summary()
 
     t_step, t_sweeps, t_e2e = max_over_ranks([t_step, t_sweeps, t_e2e])
+    if t_exact is not None:
+        t_exact = max_over_ranks([t_exact])[0]
 
     px_iters = H * W * iters * args.steps * world
     value = job_rate(H * W * iters * args.steps, world, t_step) / 1e6
@@ -773,6 +786,10 @@ def main():
                 "pipeline": "pinned host -> device -> pinned host every step; copy-in and "
                             "copy-out streams overlap step k+1's and k-1's copies with step k's "
                             "sweeps"},
+        "exact_form": (None if t_exact is None else
+                       {"value": H * W * iters * max(1, args.steps // 2) / t_exact / 1e6,
+                        "unit": UNIT, "sweeps_per_pass": Te, "rows_per_segment": sege,
+                        "note": "bit-identical to the reference's FP32 semantics"}),
         "gpu_launches": (1 + passes) * args.steps,
         "clocks": clocks,
     }

@@ -12,8 +12,13 @@
 //   - the per-step bookkeeping (copies, ring indices, stores) is spread over twice the
 //     cells, and the temporal halo (T rounded up to 4 columns each side) is a smaller share
 //     of the strip (120 or 112 output columns of 128).
-// Only the fast form (FMA, reciprocal of the denominator) exists in this layout; the exact
-// form keeps the 2-column layout, whose tap-ordered windows need 5 registers per column.
+// The arithmetic runs on column pairs with the sm_100 packed FP32 instructions (one
+// instruction, two IEEE operations rounded as their scalar forms): the pairs are columns
+// (0, 2) and (1, 3), so each pair's horizontal neighbours are the other pair plus one
+// shuffled value, and the coefficient ring holds -1/den so the update is three packed
+// FMAs and one packed multiply per pair; results equal the scalar 2-column kernel's bit for
+// bit.  Only the fast form (FMA, reciprocal of the denominator) exists in this layout; the
+// exact form keeps the 2-column layout, whose tap-ordered windows need 5 registers per column.
 #pragma once
 
 #include "hs_stream.cuh"
@@ -30,14 +35,14 @@ struct GeoW {
     static constexpr int strip = kWideCols - 2 * halo;         // output columns per strip
     static constexpr int coef_slots = T + 1;                   // rows k-T .. k
     static constexpr int raw_floats = kWideRawSlots * kRawPlanes * kWideCols;
-    static constexpr int coef_floats = coef_slots * 4 * 32 * 4;  // [slot][column][lane] float4
+    static constexpr int coef_floats = coef_slots * 4 * 32 * 4;  // [slot][4][lane] float4
     static constexpr int warp_floats = raw_floats + coef_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
 };
 
 struct ItemW {
     float *raw;     // [kWideRawSlots][kRawPlanes][128]
-    float4 *coef;   // [T+1][4][32]
+    float4 *coef;   // [T+1][4][32]: per pair (0,2) then (1,3): (Ix, Iy) then (It, -1/den)
     int lane;
     int lcol;       // this lane's chunk, clamped to an in-bounds chunk of the row
     int xa;         // first of the lane's 4 columns
@@ -62,60 +67,87 @@ __device__ __forceinline__ void issue_row_w(const ItemW &it, int slot, int row, 
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
+// Rolling 3x3 windows of two columns (a packed pair): the same recurrence as the scalar
+// Win<true> (vertical sums carried as Z, Y1), one packed instruction per operation.
+struct Win2 {
+    float2 Z, Y1;
+};
+
+template <bool EDGE>
+__device__ __forceinline__ float2 win_step2(Win2 &w, float2 l, float2 c, float2 r, int n, int H,
+                                            float2 we, float2 wc) {
+    const float2 hn = __fadd2_rn(l, r);
+    float2 yn = __ffma2_rn(we, c, __fmul2_rn(wc, hn));
+    if (EDGE && n >= H) yn = w.Y1;  // the row below H-1 is row H-1
+    const float2 out = __fadd2_rn(w.Z, yn);
+    w.Z = __ffma2_rn(we, hn, (EDGE && n == 0) ? yn : w.Y1);  // row 0's up row is row 0
+    w.Y1 = yn;
+    return out;
+}
+
 template <int T, bool XEDGE, bool EDGE>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
-                                              Win<true> (&w)[T][2][4], int k, int rslot, int cslot) {
+                                              Win2 (&w)[T][2][2], int k, int rslot, int cslot) {
     // prefetch row k + kWidePrefetch into the slot row k-1 used, then wait for row k; the
     // lane only ever reads its own copies
     issue_row_w(it, rslot == 0 ? kWideRawSlots - 1 : rslot - 1, min(k + kWidePrefetch, it.y_end - 1 + T), p);
     cp_async_wait<kWidePrefetch>();
 
-    // stage 0: unpack row k; pack its coefficients with the reciprocal denominator
+    // stage 0: unpack row k; pack its coefficients per column pair with -1/den
     const float *raw = it.raw + rslot * (kRawPlanes * kWideCols) + 4 * it.lane;
     const float4 u4 = lds4(raw), v4 = lds4(raw + kWideCols);
     {
         const float4 ix = lds4(raw + 2 * kWideCols), iy = lds4(raw + 3 * kWideCols);
         const float4 t4 = lds4(raw + 4 * kWideCols);
+        const float n0 = -rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
+        const float n1 = -rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
+        const float n2 = -rcp_approx(fmaf(iy.z, iy.z, fmaf(ix.z, ix.z, it.alpha2)));
+        const float n3 = -rcp_approx(fmaf(iy.w, iy.w, fmaf(ix.w, ix.w, it.alpha2)));
         float4 *cs = it.coef + cslot * 128 + it.lane;
-        cs[0] = make_float4(ix.x, iy.x, t4.x, rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2))));
-        cs[32] = make_float4(ix.y, iy.y, t4.y, rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2))));
-        cs[64] = make_float4(ix.z, iy.z, t4.z, rcp_approx(fmaf(iy.z, iy.z, fmaf(ix.z, ix.z, it.alpha2))));
-        cs[96] = make_float4(ix.w, iy.w, t4.w, rcp_approx(fmaf(iy.w, iy.w, fmaf(ix.w, ix.w, it.alpha2))));
+        cs[0] = make_float4(ix.x, ix.z, iy.x, iy.z);
+        cs[32] = make_float4(t4.x, t4.z, n0, n2);
+        cs[64] = make_float4(ix.y, ix.w, iy.y, iy.w);
+        cs[96] = make_float4(t4.y, t4.w, n1, n3);
     }
-    float cu[2][4] = {{u4.x, u4.y, u4.z, u4.w}, {v4.x, v4.y, v4.z, v4.w}};  // [plane][column]
+    // [plane][pair]: pair 0 holds columns (0, 2), pair 1 columns (1, 3)
+    float2 cu[2][2] = {{make_float2(u4.x, u4.z), make_float2(u4.y, u4.w)},
+                       {make_float2(v4.x, v4.z), make_float2(v4.y, v4.w)}};
+    const float2 we2 = make_float2(p.we, p.we), wc2 = make_float2(p.wc, p.wc);
 
 #pragma unroll
     for (int s = 0; s < T; ++s) {
         const int n = k - s;  // arriving row (input of sweep s+1)
-        float ub[2][4];
+        float2 ub[2][2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const float c0 = cu[q][0], c1 = cu[q][1], c2 = cu[q][2], c3 = cu[q][3];
-            float l0 = __shfl_up_sync(kFull, c3, 1);
-            float r3 = __shfl_down_sync(kFull, c0, 1);
-            float r0 = c1, r1 = c2, r2 = c3;
+            const float2 E = cu[q][0], O = cu[q][1];  // (c0, c2), (c1, c3)
+            const float lsh = __shfl_up_sync(kFull, O.y, 1);    // column -1: lane-1's c3
+            const float rsh = __shfl_down_sync(kFull, E.x, 1);  // column 4: lane+1's c0
+            float2 lE = make_float2(lsh, O.x), rE = O;          // neighbours of (c0, c2)
+            float2 rO = make_float2(E.y, rsh);                  // right of (c1, c3); left is E
             if constexpr (XEDGE) {
-                l0 = it.first ? c0 : l0;
-                r0 = (it.last & 1u) ? c0 : r0;
-                r1 = (it.last & 2u) ? c1 : r1;
-                r2 = (it.last & 4u) ? c2 : r2;
-                r3 = (it.last & 8u) ? c3 : r3;
+                lE.x = it.first ? E.x : lE.x;
+                rE.x = (it.last & 1u) ? E.x : rE.x;
+                rO.x = (it.last & 2u) ? O.x : rO.x;
+                rE.y = (it.last & 4u) ? E.y : rE.y;
+                rO.y = (it.last & 8u) ? O.y : rO.y;
             }
-            ub[q][0] = win_step<EDGE>(w[s][q][0], l0, c0, r0, n, p.H, p.we, p.wc);
-            ub[q][1] = win_step<EDGE>(w[s][q][1], c0, c1, r1, n, p.H, p.we, p.wc);
-            ub[q][2] = win_step<EDGE>(w[s][q][2], c1, c2, r2, n, p.H, p.we, p.wc);
-            ub[q][3] = win_step<EDGE>(w[s][q][3], c2, c3, r3, n, p.H, p.we, p.wc);
+            ub[q][0] = win_step2<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
+            ub[q][1] = win_step2<EDGE>(w[s][q][1], E, O, rO, n, p.H, we2, wc2);
         }
         int rs = cslot - (s + 1);
         if (rs < 0) rs += GeoW<T>::coef_slots;
         const float4 *cr = it.coef + rs * 128 + it.lane;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const float4 C = cr[32 * j];
-            const float ubar = ub[0][j], vbar = ub[1][j];
-            const float t = fmaf(C.x, ubar, fmaf(C.y, vbar, C.z)) * C.w;
-            cu[0][j] = fmaf(-C.x, t, ubar);
-            cu[1][j] = fmaf(-C.y, t, vbar);
+        for (int j = 0; j < 2; ++j) {
+            const float4 A = cr[64 * j], B = cr[64 * j + 32];
+            const float2 cx = make_float2(A.x, A.y), cy = make_float2(A.z, A.w);
+            const float2 ct = make_float2(B.x, B.y), nw = make_float2(B.z, B.w);
+            const float2 ubar = ub[0][j], vbar = ub[1][j];
+            // -t = (Ix ubar + Iy vbar + It) * (-1/den); u = ubar + Ix (-t) = ubar - Ix t
+            const float2 nt = __fmul2_rn(__ffma2_rn(cx, ubar, __ffma2_rn(cy, vbar, ct)), nw);
+            cu[0][j] = __ffma2_rn(cx, nt, ubar);
+            cu[1][j] = __ffma2_rn(cy, nt, vbar);
         }
     }
 
@@ -123,15 +155,17 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
     const int r = k - T;
     if (r >= it.y_start && r < it.y_end) {
         const size_t off = (size_t)r * p.ld + it.xa;
+        const float uo[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
+        const float vo[4] = {cu[1][0].x, cu[1][1].x, cu[1][0].y, cu[1][1].y};
         if (it.st == 15u) {
-            *reinterpret_cast<float4 *>(p.u_out + off) = make_float4(cu[0][0], cu[0][1], cu[0][2], cu[0][3]);
-            *reinterpret_cast<float4 *>(p.v_out + off) = make_float4(cu[1][0], cu[1][1], cu[1][2], cu[1][3]);
+            *reinterpret_cast<float4 *>(p.u_out + off) = make_float4(uo[0], uo[1], uo[2], uo[3]);
+            *reinterpret_cast<float4 *>(p.v_out + off) = make_float4(vo[0], vo[1], vo[2], vo[3]);
         } else if (it.st) {
 #pragma unroll
             for (int j = 0; j < 4; ++j)
                 if (it.st & (1u << j)) {
-                    p.u_out[off + j] = cu[0][j];
-                    p.v_out[off + j] = cu[1][j];
+                    p.u_out[off + j] = uo[j];
+                    p.v_out[off + j] = vo[j];
                 }
         }
     }
@@ -141,13 +175,13 @@ template <int T, bool XEDGE>
 __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
-    Win<true> w[T][2][4];
+    Win2 w[T][2][2];
 #pragma unroll
     for (int s = 0; s < T; ++s)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int j = 0; j < 4; ++j) w[s][q][j] = Win<true>{};
+            for (int j = 0; j < 2; ++j) w[s][q][j] = Win2{};
 
 #pragma unroll
     for (int i = 0; i < kWidePrefetch; ++i) issue_row_w(it, i, k0 + i, p);
