@@ -65,6 +65,37 @@ constexpr float kAvgCorner = (float)(1.0 / 12.0);
 constexpr float kAvgEdge = (float)(1.0 / 6.0);
 
 #ifdef __CUDACC__
+// Packed FP32 pairs (sm_100 f32x2 instructions: one instruction, two IEEE operations, each
+// rounded to nearest even as its scalar form).
+//   add2 / fma2: packed add and fused multiply-add.
+//   mul2       : packed product, only where it feeds no add: the code generator fuses a
+//                packed product into a following packed add (an FMA, which skips the
+//                product's rounding) even with explicit .rn;
+//   mul2r      : the product rounded on its own, as two scalar multiplies (never fused),
+//                for the exact operation order.
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+        "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+    float2 d;
+    asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+        "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+        "mul.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+        : "=f"(d.x), "=f"(d.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return d;
+}
+__device__ __forceinline__ float2 mul2r(float2 a, float2 b) {
+    return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 // Horn-Schunck 2x2x2 derivatives at (x, y).  Tap order (0,0) (1,0) (0,1) (1,1), taps
 // clamped to the image; each accumulator sums from 0 in that order, one rounding per
 // operation; then Ix = DxI0 + DxI1, Iy = DyI0 + DyI1, It = DtI1 - DtI0.

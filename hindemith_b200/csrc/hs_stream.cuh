@@ -10,8 +10,12 @@
 //   - vertical neighbours come from a rolling window kept in registers (2 values per
 //     column and plane in the fast form, tap-ordered accumulators in the exact form),
 //   - the rows (u, v, Ix, Iy, It) arrive in a per-warp shared-memory ring through 16-byte
-//     cp.async copies three rows ahead; stage 0 repacks each column's coefficients with
-//     the per-pixel denominator term as one float4 for the stages to read.
+//     cp.async copies three rows ahead; stage 0 repacks the lane's coefficients (Ix, Iy,
+//     It and the negated denominator term, each as a column pair) for the stages to read,
+//   - the lane's two columns are one packed FP32 pair: the sm_100 f32x2 instructions do
+//     both columns' operation in one instruction, each rounded as its scalar form, so the
+//     results are those of the scalar operation sequence bit for bit (the exact form's
+//     products stay scalar multiplies, which are never fused into the adds).
 // A strip loads `halo` extra columns each side (T rounded up to a multiple of 4) and
 // outputs the middle 64 - 2*halo; a segment starts T rows early; both are the temporal
 // blocking halo.  Warps never synchronise with each other; within a warp, a barrier after
@@ -51,7 +55,7 @@ struct Geo {
     static constexpr int strip = kWarpCols - 2 * halo;         // output columns per strip
     static constexpr int coef_slots = T + 1;                   // rows k-T .. k
     static constexpr int raw_floats = kRawSlots * kRawPlanes * rw;
-    static constexpr int coef_floats = coef_slots * 2 * 32 * 4;  // [slot][column][lane] float4
+    static constexpr int coef_floats = coef_slots * 2 * 32 * 4;  // [slot][2][lane] float4
     static constexpr int warp_floats = raw_floats + coef_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
 };
@@ -100,10 +104,13 @@ __device__ __forceinline__ float rcp_approx(float x) {
 
 __device__ __forceinline__ float2 lds2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
 
-// Sliding three-row window of one stage, one plane, one column.
+__device__ __forceinline__ float2 f2(float x, float y) { return make_float2(x, y); }
+
+// Sliding three-row window of one stage and one plane, for a pair of columns (the
+// vertical recurrences are per column, so two columns run as one packed pair).
 //   fast : with Y(k) = we*c(k) + wc*h(k) (h = left + right), the average of row n-1 is
 //          Y(n-2) + we*h(n-1) + Y(n).  Z = Y(n-2) + we*h(n-1) and Y1 = Y(n-1) are kept,
-//          so a row costs 5 operations and 2 registers.
+//          so a row costs 5 operations and 2 registers per column.
 //   exact: A0 = next row's accumulator holding its up taps (taken from row n-1),
 //          A1 = row n-1's accumulator holding its up and mid taps, l1/c1/r1 = row n-1
 //          (read only for the bottom clamp)
@@ -111,43 +118,45 @@ template <bool FAST>
 struct Win;
 template <>
 struct Win<true> {
-    float Z, Y1;
+    float2 Z, Y1;
 };
 template <>
 struct Win<false> {
-    float A0, A1, l1, c1, r1;
+    float2 A0, A1, l1, c1, r1;
 };
 
-// Row n arrives (values l, c, r at this column); returns the average of row n-1 and
-// advances the window.  EDGE: the row may be row 0 (top clamp) or past the bottom
-// (replaced by row H-1, the bottom clamp).
+// Row n arrives (values l, c, r at the pair's columns); returns the average of row n-1
+// and advances the window.  EDGE: the row may be row 0 (top clamp) or past the bottom
+// (replaced by row H-1, the bottom clamp).  The fast form has no product feeding an add
+// (mul2's restriction).
 template <bool EDGE>
-__device__ __forceinline__ float win_step(Win<true> &w, float l, float c, float r, int n, int H,
-                                          float we, float wc) {
-    const float hn = l + r;
-    float yn = fmaf(we, c, wc * hn);
+__device__ __forceinline__ float2 win_step(Win<true> &w, float2 l, float2 c, float2 r, int n, int H,
+                                           float2 we, float2 wc) {
+    const float2 hn = add2(l, r);
+    float2 yn = fma2(we, c, mul2(wc, hn));
     if (EDGE && n >= H) yn = w.Y1;  // the row below H-1 is row H-1
-    const float out = w.Z + yn;
-    w.Z = fmaf(we, hn, (EDGE && n == 0) ? yn : w.Y1);  // row 0's up row is row 0
+    const float2 out = add2(w.Z, yn);
+    w.Z = fma2(we, hn, (EDGE && n == 0) ? yn : w.Y1);  // row 0's up row is row 0
     w.Y1 = yn;
     return out;
 }
 
 template <bool EDGE>
-__device__ __forceinline__ float win_step(Win<false> &w, float l, float c, float r, int n, int H,
-                                          float we, float wc) {
+__device__ __forceinline__ float2 win_step(Win<false> &w, float2 l, float2 c, float2 r, int n, int H,
+                                           float2 we, float2 wc) {
     if (EDGE && n >= H) { l = w.l1; c = w.c1; r = w.r1; }
     // taps in row-major order: (-1,-1) (0,-1) (1,-1) | (-1,0) (1,0) | (-1,1) (0,1) (1,1)
-    float o = w.A1;                              // row n-1: up and mid taps done
-    o = __fadd_rn(o, __fmul_rn(wc, l));          // its dn taps come from row n
-    o = __fadd_rn(o, __fmul_rn(we, c));
-    o = __fadd_rn(o, __fmul_rn(wc, r));
-    float up = __fadd_rn(0.0f, __fmul_rn(wc, l));  // row n+1's up taps come from row n
-    up = __fadd_rn(up, __fmul_rn(we, c));
-    up = __fadd_rn(up, __fmul_rn(wc, r));
-    float am = (EDGE && n == 0) ? up : w.A0;     // row 0's up taps are its own (clamp)
-    am = __fadd_rn(am, __fmul_rn(we, l));        // row n's mid taps
-    am = __fadd_rn(am, __fmul_rn(we, r));
+    const float2 tl = mul2r(wc, l), tc = mul2r(we, c), tr = mul2r(wc, r);
+    float2 o = w.A1;                              // row n-1: up and mid taps done
+    o = add2(o, tl);                              // its dn taps come from row n
+    o = add2(o, tc);
+    o = add2(o, tr);
+    float2 up = add2(f2(0.0f, 0.0f), tl);         // row n+1's up taps come from row n
+    up = add2(up, tc);
+    up = add2(up, tr);
+    float2 am = (EDGE && n == 0) ? up : w.A0;     // row 0's up taps are its own (clamp)
+    am = add2(am, mul2r(we, l));                  // row n's mid taps
+    am = add2(am, mul2r(we, r));
     w.A0 = up;
     w.A1 = am;
     if (EDGE) { w.l1 = l; w.c1 = c; w.r1 = r; }
@@ -157,7 +166,7 @@ __device__ __forceinline__ float win_step(Win<false> &w, float l, float c, float
 // Per-warp context of one work item.
 struct Item {
     float *raw;    // [kRawSlots][kRawPlanes][64] floats
-    float4 *coef;  // [T+1][2][32]
+    float4 *coef;  // [T+1][2][32]: (Ix, Iy) then (It, -den term) as column pairs
     int lane;
     int lcol;      // first column of this lane's 16-byte chunk (clamped into the row)
     int lc2;       // the lane's own column pair (xa, xa+1), or any in-bounds pair
@@ -198,7 +207,7 @@ __device__ __forceinline__ void issue_row(const Item &it, int slot, int row, con
 
 // One streaming step: row k arrives at stage 0, stage s emits sweep s+1 of row k-s-1.
 template <int T, bool FAST, bool XEDGE, bool EDGE, bool DUMP>
-__device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it, Win<FAST> (&w)[T][2][2],
+__device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it, Win<FAST> (&w)[T][2],
                                             int k, int rslot, int cslot) {
     // Prefetch row k + kPrefetch into the slot row k-1 used, then wait for row k (never
     // beyond the item's last row: rows past it may belong to tiles that a later pass is
@@ -212,76 +221,74 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     cp_async_wait<kPrefetch>();
     __syncwarp();
 
-    // stage 0: unpack row k; pack its coefficients with the denominator term
+    // stage 0: unpack row k; pack its coefficients with the negated denominator term
+    // (-1/den in the fast form, -den in the exact one: the update then adds a product)
     constexpr int RW = Geo<T>::rw;
     const float *raw = it.raw + rslot * (kRawPlanes * RW) + Geo<T>::sh + 2 * it.lane;
-    const float2 u2 = lds2(raw), v2 = lds2(raw + RW);
+    float2 cu[2] = {lds2(raw), lds2(raw + RW)};  // [plane]: the lane's (u, v) column pairs
     {
         const float2 ix = lds2(raw + 2 * RW), iy = lds2(raw + 3 * RW);
         const float2 t2 = lds2(raw + 4 * RW);
-        float ax, ay;
+        float2 nd;
         if constexpr (FAST) {
-            ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
-            ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
+            nd = f2(-rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2))),
+                    -rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2))));
         } else {
-            ax = __fadd_rn(__fadd_rn(it.alpha2, __fmul_rn(ix.x, ix.x)), __fmul_rn(iy.x, iy.x));
-            ay = __fadd_rn(__fadd_rn(it.alpha2, __fmul_rn(ix.y, ix.y)), __fmul_rn(iy.y, iy.y));
+            const float2 d = add2(add2(f2(it.alpha2, it.alpha2), mul2r(ix, ix)), mul2r(iy, iy));
+            nd = f2(-d.x, -d.y);
         }
         float4 *cs = it.coef + cslot * 64 + it.lane;
-        cs[0] = make_float4(ix.x, iy.x, t2.x, ax);
-        cs[32] = make_float4(ix.y, iy.y, t2.y, ay);
+        cs[0] = make_float4(ix.x, ix.y, iy.x, iy.y);
+        cs[32] = make_float4(t2.x, t2.y, nd.x, nd.y);
     }
-    float cu[2][2] = {{u2.x, u2.y}, {v2.x, v2.y}};  // [plane][column]
+    const float2 we2 = f2(p.we, p.we), wc2 = f2(p.wc, p.wc);
 
 #pragma unroll
     for (int s = 0; s < T; ++s) {
         const int n = k - s;  // arriving row (input of sweep s+1)
-        float ub[2][2];
+        float2 ub[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const float ca = cu[q][0], cb = cu[q][1];
-            const float fromL = __shfl_up_sync(kFull, cb, 1);
-            const float fromR = __shfl_down_sync(kFull, ca, 1);
-            float la = fromL, ra = cb, rb = fromR;
+            const float2 c = cu[q];
+            const float fromL = __shfl_up_sync(kFull, c.y, 1);
+            const float fromR = __shfl_down_sync(kFull, c.x, 1);
+            float2 l = f2(fromL, c.x), r = f2(c.y, fromR);
             if constexpr (XEDGE) {
-                la = it.a_first ? ca : la;
-                ra = it.a_last ? ca : ra;
-                rb = it.b_last ? cb : rb;
+                l.x = it.a_first ? c.x : l.x;
+                r.x = it.a_last ? c.x : r.x;
+                r.y = it.b_last ? c.y : r.y;
             }
-            ub[q][0] = win_step<EDGE>(w[s][q][0], la, ca, ra, n, p.H, p.we, p.wc);
-            ub[q][1] = win_step<EDGE>(w[s][q][1], ca, cb, rb, n, p.H, p.we, p.wc);
+            ub[q] = win_step<EDGE>(w[s][q], l, c, r, n, p.H, we2, wc2);
         }
         // pointwise update of row n-1 with its coefficients
         int rs = cslot - (s + 1);
         if (rs < 0) rs += Geo<T>::coef_slots;
         const float4 *cr = it.coef + rs * 64 + it.lane;
-        const float4 C[2] = {cr[0], cr[32]};
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const float ubar = ub[0][j], vbar = ub[1][j];
-            if constexpr (FAST) {
-                const float r = fmaf(C[j].x, ubar, fmaf(C[j].y, vbar, C[j].z));
-                const float t = r * C[j].w;
-                cu[0][j] = fmaf(-C[j].x, t, ubar);
-                cu[1][j] = fmaf(-C[j].y, t, vbar);
-            } else {
-                float r = __fadd_rn(__fmul_rn(C[j].x, ubar), __fmul_rn(C[j].y, vbar));
-                r = __fadd_rn(r, C[j].z);
-                const float t = __fdiv_rn(r, C[j].w);
-                cu[0][j] = __fsub_rn(ubar, __fmul_rn(C[j].x, t));
-                cu[1][j] = __fsub_rn(vbar, __fmul_rn(C[j].y, t));
-            }
+        const float4 A = cr[0], B = cr[32];
+        const float2 cx = f2(A.x, A.y), cy = f2(A.z, A.w), ct = f2(B.x, B.y), nd = f2(B.z, B.w);
+        const float2 ubar = ub[0], vbar = ub[1];
+        if constexpr (FAST) {
+            // -t = (Ix ubar + Iy vbar + It) * (-1/den); u = ubar + Ix (-t) = ubar - Ix t
+            const float2 nt = mul2(fma2(cx, ubar, fma2(cy, vbar, ct)), nd);
+            cu[0] = fma2(cx, nt, ubar);
+            cu[1] = fma2(cy, nt, vbar);
+        } else {
+            // t = ((Ix ubar + Iy vbar) + It) / den and u = ubar - Ix t, with -t = r / (-den)
+            const float2 r = add2(add2(mul2r(cx, ubar), mul2r(cy, vbar)), ct);
+            const float2 nt = f2(__fdiv_rn(r.x, nd.x), __fdiv_rn(r.y, nd.y));
+            cu[0] = add2(ubar, mul2r(cx, nt));
+            cu[1] = add2(vbar, mul2r(cy, nt));
         }
         if constexpr (DUMP) {  // write sweep s+1 of row k-s-1 (state dumps)
             const int rr = k - s - 1;
             if (rr >= it.y_start && rr < it.y_end) {
                 const size_t off = (size_t)rr * p.ld + it.xa;
                 if (it.st_a && it.st_b) {
-                    *reinterpret_cast<float2 *>(p.dump_u[s] + off) = make_float2(cu[0][0], cu[0][1]);
-                    *reinterpret_cast<float2 *>(p.dump_v[s] + off) = make_float2(cu[1][0], cu[1][1]);
+                    *reinterpret_cast<float2 *>(p.dump_u[s] + off) = cu[0];
+                    *reinterpret_cast<float2 *>(p.dump_v[s] + off) = cu[1];
                 } else if (it.st_a) {
-                    p.dump_u[s][off] = cu[0][0];
-                    p.dump_v[s][off] = cu[1][0];
+                    p.dump_u[s][off] = cu[0].x;
+                    p.dump_v[s][off] = cu[1].x;
                 }
             }
         }
@@ -292,11 +299,11 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     if (r >= it.y_start && r < it.y_end) {
         const size_t off = (size_t)r * p.ld + it.xa;
         if (it.st_a && it.st_b) {
-            *reinterpret_cast<float2 *>(p.u_out + off) = make_float2(cu[0][0], cu[0][1]);
-            *reinterpret_cast<float2 *>(p.v_out + off) = make_float2(cu[1][0], cu[1][1]);
+            *reinterpret_cast<float2 *>(p.u_out + off) = cu[0];
+            *reinterpret_cast<float2 *>(p.v_out + off) = cu[1];
         } else if (it.st_a) {
-            p.u_out[off] = cu[0][0];
-            p.v_out[off] = cu[1][0];
+            p.u_out[off] = cu[0].x;
+            p.v_out[off] = cu[1].x;
         }
     }
 }
@@ -305,13 +312,11 @@ template <int T, bool FAST, bool XEDGE, bool DUMP>
 __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
-    Win<FAST> w[T][2][2];
+    Win<FAST> w[T][2];
 #pragma unroll
     for (int s = 0; s < T; ++s)
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) w[s][q][j] = Win<FAST>{};
+        for (int q = 0; q < 2; ++q) w[s][q] = Win<FAST>{};
 
 #pragma unroll
     for (int i = 0; i < kPrefetch; ++i) issue_row<T>(it, i, k0 + i, p);
@@ -340,9 +345,7 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
 #pragma unroll
             for (int s = 0; s < T; ++s)
 #pragma unroll
-                for (int q = 0; q < 2; ++q)
-#pragma unroll
-                    for (int j = 0; j < 2; ++j) w[s][q][j].l1 = w[s][q][j].c1 = w[s][q][j].r1 = 0.f;
+                for (int q = 0; q < 2; ++q) w[s][q].l1 = w[s][q].c1 = w[s][q].r1 = f2(0.f, 0.f);
         }
     }
     for (; k <= k_end; advance()) stream_step<T, FAST, XEDGE, true, DUMP>(p, it, w, k, rslot, cslot);

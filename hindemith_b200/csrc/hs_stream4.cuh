@@ -67,27 +67,9 @@ __device__ __forceinline__ void issue_row_w(const ItemW &it, int slot, int row, 
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-// Rolling 3x3 windows of two columns (a packed pair): the same recurrence as the scalar
-// Win<true> (vertical sums carried as Z, Y1), one packed instruction per operation.
-struct Win2 {
-    float2 Z, Y1;
-};
-
-template <bool EDGE>
-__device__ __forceinline__ float2 win_step2(Win2 &w, float2 l, float2 c, float2 r, int n, int H,
-                                            float2 we, float2 wc) {
-    const float2 hn = __fadd2_rn(l, r);
-    float2 yn = __ffma2_rn(we, c, __fmul2_rn(wc, hn));
-    if (EDGE && n >= H) yn = w.Y1;  // the row below H-1 is row H-1
-    const float2 out = __fadd2_rn(w.Z, yn);
-    w.Z = __ffma2_rn(we, hn, (EDGE && n == 0) ? yn : w.Y1);  // row 0's up row is row 0
-    w.Y1 = yn;
-    return out;
-}
-
 template <int T, bool XEDGE, bool EDGE>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
-                                              Win2 (&w)[T][2][2], int k, int rslot, int cslot) {
+                                              Win<true> (&w)[T][2][2], int k, int rslot, int cslot) {
     // prefetch row k + kWidePrefetch into the slot row k-1 used, then wait for row k; the
     // lane only ever reads its own copies
     issue_row_w(it, rslot == 0 ? kWideRawSlots - 1 : rslot - 1, min(k + kWidePrefetch, it.y_end - 1 + T), p);
@@ -132,8 +114,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
                 rE.y = (it.last & 4u) ? E.y : rE.y;
                 rO.y = (it.last & 8u) ? O.y : rO.y;
             }
-            ub[q][0] = win_step2<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
-            ub[q][1] = win_step2<EDGE>(w[s][q][1], E, O, rO, n, p.H, we2, wc2);
+            ub[q][0] = win_step<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
+            ub[q][1] = win_step<EDGE>(w[s][q][1], E, O, rO, n, p.H, we2, wc2);
         }
         int rs = cslot - (s + 1);
         if (rs < 0) rs += GeoW<T>::coef_slots;
@@ -145,9 +127,9 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             const float2 ct = make_float2(B.x, B.y), nw = make_float2(B.z, B.w);
             const float2 ubar = ub[0][j], vbar = ub[1][j];
             // -t = (Ix ubar + Iy vbar + It) * (-1/den); u = ubar + Ix (-t) = ubar - Ix t
-            const float2 nt = __fmul2_rn(__ffma2_rn(cx, ubar, __ffma2_rn(cy, vbar, ct)), nw);
-            cu[0][j] = __ffma2_rn(cx, nt, ubar);
-            cu[1][j] = __ffma2_rn(cy, nt, vbar);
+            const float2 nt = mul2(fma2(cx, ubar, fma2(cy, vbar, ct)), nw);
+            cu[0][j] = fma2(cx, nt, ubar);
+            cu[1][j] = fma2(cy, nt, vbar);
         }
     }
 
@@ -175,13 +157,13 @@ template <int T, bool XEDGE>
 __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
-    Win2 w[T][2][2];
+    Win<true> w[T][2][2];
 #pragma unroll
     for (int s = 0; s < T; ++s)
 #pragma unroll
         for (int q = 0; q < 2; ++q)
 #pragma unroll
-            for (int j = 0; j < 2; ++j) w[s][q][j] = Win2{};
+            for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
 
 #pragma unroll
     for (int i = 0; i < kWidePrefetch; ++i) issue_row_w(it, i, k0 + i, p);

@@ -167,7 +167,7 @@ __device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, i
 
 template <int TB, bool XEDGE, bool EDGE>
 __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp, const Item &it,
-                                         float4 *ring, Win<true> (&w)[TB][2][2], float inv_a2,
+                                         float4 *ring, Win<true> (&w)[TB][2], float inv_a2,
                                          float we, float wc, int k, int rslot, int cslot,
                                          float2 (&xs)[TB][2], float &a2s) {
     __syncwarp();
@@ -203,17 +203,18 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
         float lam[2][2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const float ca = cu[q][0], cb = cu[q][1];
-            const float fromL = __shfl_up_sync(kFull, cb, 1);
-            const float fromR = __shfl_down_sync(kFull, ca, 1);
-            float la = fromL, ra = cb, rb = fromR;
+            const float2 c = f2(cu[q][0], cu[q][1]);
+            const float fromL = __shfl_up_sync(kFull, c.y, 1);
+            const float fromR = __shfl_down_sync(kFull, c.x, 1);
+            float2 l = f2(fromL, c.x), r = f2(c.y, fromR);
             if constexpr (XEDGE) {
-                la = it.a_first ? ca : la;
-                ra = it.a_last ? ca : ra;
-                rb = it.b_last ? cb : rb;
+                l.x = it.a_first ? c.x : l.x;
+                r.x = it.a_last ? c.x : r.x;
+                r.y = it.b_last ? c.y : r.y;
             }
-            lam[q][0] = win_step<EDGE>(w[s - 1][q][0], la, ca, ra, n, P.H, we, wc);
-            lam[q][1] = win_step<EDGE>(w[s - 1][q][1], ca, cb, rb, n, P.H, we, wc);
+            const float2 m = win_step<EDGE>(w[s - 1][q], l, c, r, n, P.H, f2(we, we), f2(wc, wc));
+            lam[q][0] = m.x;
+            lam[q][1] = m.y;
         }
         if (s < TB) {  // M of the next sweep at row k - s
             int rs = cslot - s;
@@ -283,13 +284,11 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
     const float inv_a2 = 1.0f / (a * a);
     const int k0 = max(0, it.y_start - TB);
     const int k_end = it.y_end - 1 + TB;
-    Win<true> w[TB][2][2];
+    Win<true> w[TB][2];
 #pragma unroll
     for (int s = 0; s < TB; ++s)
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
+        for (int q = 0; q < 2; ++q) w[s][q] = Win<true>{};
 #pragma unroll
     for (int i = 0; i < kPrefetch; ++i) issue_row<TB>(it, i, k0 + i, lp);
     float2 xs[TB][2];
