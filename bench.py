@@ -494,8 +494,15 @@ def measure_fusion_flow(args, rank, flush, peak):
         p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
     t = timed_events(lambda: FL.lk_least_squares(err, Ix, Iy, 5), k, 3, flush, stream, "timed_lk")
     lk_flops = H * W * (2 * 5) ** 2 * 10
+    # The window sums' adds are fixed by the reference order (5 per window cell, 100 cells);
+    # they bound the kernel on the FP32 pipe (128 lanes per SM per clock).
+    lk_adds = H * W * (2 * 5) ** 2 * 5
+    fp32_peak = torch.cuda.get_device_properties(0).multi_processor_count * 128 * 1965e6
     out["lk"] = {"workload": "lk_least_squares_1920x1080_radius5", "ms": t / k * 1e3,
-                 "gflops": lk_flops * k / t / 1e9, "bound": "fp32 issue"}
+                 "gflops": lk_flops * k / t / 1e9, "bound": "fp32 pipe",
+                 "roofline": {"order_fixed_adds_per_px": 500, "achieved_tops": lk_adds * k / t / 1e12,
+                              "peak_tops": fp32_peak / 1e12, "frac": lk_adds * k / t / fp32_peak,
+                              "peak_source": "SMs x 128 FP32 lanes x clocks.max.sm (1965 MHz)"}}
     Hb = Wb = 2048
     psi, x, d0, d1, od = D.empty_planes(5, Hb, Wb)
     for p in (psi, x, d0, d1, od):

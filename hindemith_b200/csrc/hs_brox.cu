@@ -9,23 +9,43 @@
 
 namespace hs {
 
-constexpr int kLkTile = 32;      // output tile edge
+constexpr int kLkCols = 32;      // output columns per CTA (one per lane)
+constexpr int kLkWarps = 4;      // warps per CTA, stacked vertically
 constexpr int kLkMaxRadius = 16;
 
-// LKLeastSquares.cpp:44-79.  A 32 x 32 output tile per CTA (32 x 8 threads, 4 rows each);
-// Ix, Iy and the error image are staged in shared memory with a halo of `rad` cells.
-__global__ void __launch_bounds__(256) lk_kernel(const float *__restrict__ err,
-                                                 const float *__restrict__ Ix,
-                                                 const float *__restrict__ Iy, int H, int W,
-                                                 int ld, int rad, float *__restrict__ du,
-                                                 float *__restrict__ dv) {
-    extern __shared__ float sm[];
-    const int E = kLkTile + 2 * rad;
-    float *sx = sm, *sy = sm + E * E, *se = sm + 2 * E * E;
-    const int tx0 = blockIdx.x * kLkTile - rad, ty0 = blockIdx.y * kLkTile - rad;
-    const int t = threadIdx.y * 32 + threadIdx.x;
-    for (int c = t; c < E * E; c += 256) {
-        const int x = tx0 + c % E, y = ty0 + c / E;
+// The five products of one window cell c = (Ix, Iy, err, err), each rounded once:
+// (Ix^2, Iy^2) and (Ix err, Iy err) as packed pairs, Ix Iy alone.
+struct LkProd {
+    float2 sq, et;
+    float ab;
+};
+__device__ __forceinline__ LkProd lk_prod(float4 c) {
+    const float2 xy = make_float2(c.x, c.y);
+    return {mul2r(xy, xy), mul2r(xy, make_float2(c.z, c.w)), __fmul_rn(c.x, c.y)};
+}
+
+// LKLeastSquares.cpp:44-79.  Each pixel's five window sums run over dx in [-r, r) (outer)
+// and dy in [-r, r) (inner), one rounding per operation, from 0.  A thread owns P
+// vertically adjacent pixels of one column: it walks the cell columns dx and, in each, the
+// P + 2r - 1 cell rows that the P windows cover, top to bottom, adding each cell's
+// products to the pixels whose window holds that row.  Every pixel thus sees its cells in
+// exactly the reference order, while a cell's products are formed once for up to P
+// pixels.  The (Ix^2, Iy^2) and (Ix It, Iy It) sums are packed pairs.  Needs P - 1 <= 2r.
+// The CTA stages its (32 + 2r) x (4P + 2r) cells as float4 (Ix, Iy, err, err) in shared
+// memory; cells outside the image read 0 and feed only border pixels, whose flow is 0.
+template <int P>
+__global__ void __launch_bounds__(kLkCols * kLkWarps) lk_kernel(const float *__restrict__ err,
+                                                                const float *__restrict__ Ix,
+                                                                const float *__restrict__ Iy, int H,
+                                                                int W, int ld, int rad,
+                                                                float *__restrict__ du,
+                                                                float *__restrict__ dv) {
+    extern __shared__ float4 lk_cells[];
+    const int ex = kLkCols + 2 * rad, ey = kLkWarps * P + 2 * rad;
+    const int tx0 = blockIdx.x * kLkCols - rad, ty0 = blockIdx.y * (kLkWarps * P) - rad;
+    const int t = threadIdx.y * kLkCols + threadIdx.x;
+    for (int c = t; c < ex * ey; c += kLkCols * kLkWarps) {
+        const int x = tx0 + c % ex, y = ty0 + c / ex;
         float a = 0.f, b = 0.f, e = 0.f;
         if (x >= 0 && x < W && y >= 0 && y < H) {
             const size_t o = (size_t)y * ld + x;
@@ -33,30 +53,65 @@ __global__ void __launch_bounds__(256) lk_kernel(const float *__restrict__ err,
             b = __ldg(Iy + o);
             e = __ldg(err + o);
         }
-        sx[c] = a;
-        sy[c] = b;
-        se[c] = e;
+        lk_cells[c] = make_float4(a, b, e, e);
     }
     __syncthreads();
-    const int x = blockIdx.x * kLkTile + threadIdx.x;
-    for (int r = 0; r < 4; ++r) {
-        const int y = blockIdx.y * kLkTile + threadIdx.y + 8 * r;
-        if (x >= W || y >= H) continue;
-        float u = 0.f, v = 0.f;
-        if (x >= rad && y >= rad && x <= W - rad - 1 && y <= H - rad - 1) {
-            float ix2 = 0.f, iy2 = 0.f, ixiy = 0.f, ixit = 0.f, iyit = 0.f;
-            const int cx = x - tx0, cy = y - ty0;
-            for (int dx = -rad; dx < rad; ++dx) {
-                for (int dy = -rad; dy < rad; ++dy) {
-                    const int c = (cy + dy) * E + (cx + dx);
-                    const float a = sx[c], b = sy[c], e = se[c];
-                    ix2 = __fadd_rn(ix2, __fmul_rn(a, a));
-                    iy2 = __fadd_rn(iy2, __fmul_rn(b, b));
-                    ixiy = __fadd_rn(ixiy, __fmul_rn(a, b));
-                    ixit = __fadd_rn(ixit, __fmul_rn(a, e));
-                    iyit = __fadd_rn(iyit, __fmul_rn(b, e));
+
+    const int lane = threadIdx.x, warp = threadIdx.y;
+    float2 sq[P], et[P];
+    float ab[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        sq[p] = et[p] = make_float2(0.f, 0.f);
+        ab[p] = 0.f;
+    }
+    // pixel p (row warp*P + p of the CTA's outputs) has its window rows at cell rows
+    // warp*P + p + [0, 2r) and its window columns at cell columns lane + [0, 2r)
+    const float4 *col = lk_cells + (warp * P) * ex + lane;
+    for (int dxi = 0; dxi < 2 * rad; ++dxi, ++col) {
+#pragma unroll
+        for (int j = 0; j < P - 1; ++j) {  // rows 0 .. P-2: pixels 0 .. j
+            const LkProd q = lk_prod(col[j * ex]);
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                if (p <= j) {
+                    sq[p] = add2(sq[p], q.sq);
+                    et[p] = add2(et[p], q.et);
+                    ab[p] = __fadd_rn(ab[p], q.ab);
                 }
+        }
+        for (int j = P - 1; j < 2 * rad; ++j) {  // rows P-1 .. 2r-1: every pixel
+            const LkProd q = lk_prod(col[j * ex]);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                sq[p] = add2(sq[p], q.sq);
+                et[p] = add2(et[p], q.et);
+                ab[p] = __fadd_rn(ab[p], q.ab);
             }
+        }
+#pragma unroll
+        for (int k = 0; k < P - 1; ++k) {  // rows 2r .. 2r+P-2: pixels k+1 .. P-1
+            const LkProd q = lk_prod(col[(2 * rad + k) * ex]);
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                if (p > k) {
+                    sq[p] = add2(sq[p], q.sq);
+                    et[p] = add2(et[p], q.et);
+                    ab[p] = __fadd_rn(ab[p], q.ab);
+                }
+        }
+    }
+
+    const int x = blockIdx.x * kLkCols + lane;
+    if (x >= W) return;
+    const bool xin = x >= rad && x <= W - rad - 1;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int y = blockIdx.y * (kLkWarps * P) + warp * P + p;
+        if (y >= H) break;
+        float u = 0.f, v = 0.f;
+        if (xin && y >= rad && y <= H - rad - 1) {
+            const float ix2 = sq[p].x, iy2 = sq[p].y, ixit = et[p].x, iyit = et[p].y, ixiy = ab[p];
             const float det = __fsub_rn(__fmul_rn(ix2, iy2), __fmul_rn(ixiy, ixiy));
             if (det != 0.f) {
                 u = __fdiv_rn(__fsub_rn(__fmul_rn(ixit, iy2), __fmul_rn(ixiy, iyit)), det);
@@ -67,6 +122,24 @@ __global__ void __launch_bounds__(256) lk_kernel(const float *__restrict__ err,
         du[o] = u;
         dv[o] = v;
     }
+}
+
+template <int P>
+hs_status launch_lk(const float *err, const float *Ix, const float *Iy, int H, int W, int ld,
+                    int rad, float *du, float *dv, cudaStream_t s) {
+    static bool attr[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        const int max_smem = (kLkCols + 2 * kLkMaxRadius) * (kLkWarps * P + 2 * kLkMaxRadius) * 16;
+        HS_CUDA_CHECK(cudaFuncSetAttribute(lk_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_smem));
+        attr[dev] = true;
+    }
+    const int smem = (kLkCols + 2 * rad) * (kLkWarps * P + 2 * rad) * 16;
+    const dim3 grid((unsigned)((W + kLkCols - 1) / kLkCols), (unsigned)((H + kLkWarps * P - 1) / (kLkWarps * P)));
+    lk_kernel<P><<<grid, dim3(kLkCols, kLkWarps), smem, s>>>(err, Ix, Iy, H, W, ld, rad, du, dv);
+    HS_LAUNCH_CHECK("lk_kernel");
+    return HS_OK;
 }
 
 // SetBroxMatrix.cpp:38-80 / SetBroxRedblackMatrix.cpp:38-80.  Each diagonal is indexed by
@@ -172,20 +245,11 @@ hs_status hs_lk_least_squares(const float *err, const float *Ix, const float *Iy
         if ((st = check_plane(pl[k], nm[k])) != HS_OK) return st;
     if (radius < 1 || radius > kLkMaxRadius)
         HS_FAIL(HS_ERR_INVALID_ARG, "radius=%d outside 1..%d", radius, kLkMaxRadius);
-    const int E = kLkTile + 2 * radius;
-    const int smem = 3 * E * E * (int)sizeof(float);
-    static bool attr[64] = {};
-    int dev = 0;
-    HS_CUDA_CHECK(cudaGetDevice(&dev));
-    if (dev < 64 && !attr[dev]) {
-        HS_CUDA_CHECK(cudaFuncSetAttribute(lk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           3 * (kLkTile + 2 * kLkMaxRadius) * (kLkTile + 2 * kLkMaxRadius) * (int)sizeof(float)));
-        attr[dev] = true;
-    }
-    const dim3 grid((unsigned)((W + kLkTile - 1) / kLkTile), (unsigned)((H + kLkTile - 1) / kLkTile));
-    lk_kernel<<<grid, dim3(32, 8), smem, (cudaStream_t)stream>>>(err, Ix, Iy, H, W, ld, radius, du, dv);
-    HS_LAUNCH_CHECK("lk_kernel");
-    return HS_OK;
+    // pixels per thread: 8, or fewer where a window is shorter than 7 rows
+    cudaStream_t s = (cudaStream_t)stream;
+    if (radius >= 4) return launch_lk<8>(err, Ix, Iy, H, W, ld, radius, du, dv, s);
+    if (radius >= 2) return launch_lk<4>(err, Ix, Iy, H, W, ld, radius, du, dv, s);
+    return launch_lk<2>(err, Ix, Iy, H, W, ld, radius, du, dv, s);
 }
 
 hs_status hs_set_brox_matrix(const float *psi, int H, int W, int ld, float alpha, float *data,

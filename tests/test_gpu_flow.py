@@ -19,7 +19,8 @@ def cuda32(a):
 
 
 @pytest.mark.parametrize("shape,rad", [((1, 1), 1), ((9, 9), 2), ((40, 70), 5), ((131, 97), 3),
-                                       ((64, 64), 16)])
+                                       ((64, 64), 16), ((200, 150), 1), ((77, 45), 4),
+                                       ((33, 129), 7), ((300, 517), 5), ((96, 100), 16)])
 def test_lk_bitexact(cuda, shape, rad):
     H, W = shape
     rng = np.random.default_rng(H + W + rad)
