@@ -67,9 +67,12 @@ __device__ __forceinline__ void issue_row_w(const ItemW &it, int slot, int row, 
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-template <int T, bool XEDGE, bool EDGE>
+// HEAD: one of the first 2T-2 steps of a segment that starts T or more rows below the
+// image top; stage s only runs from its segment step kk = k - k0 = 2s on (see stream_item_w).
+template <int T, bool XEDGE, bool EDGE, bool HEAD = false>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
-                                              Win<true> (&w)[T][2][2], int k, int rslot, int cslot) {
+                                              Win<true> (&w)[T][2][2], int k, int rslot, int cslot,
+                                              int kk = 0) {
     // prefetch row k + kWidePrefetch into the slot row k-1 used, then wait for row k; the
     // lane only ever reads its own copies
     issue_row_w(it, rslot == 0 ? kWideRawSlots - 1 : rslot - 1, min(k + kWidePrefetch, it.y_end - 1 + T), p);
@@ -98,6 +101,7 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
 
 #pragma unroll
     for (int s = 0; s < T; ++s) {
+        if (HEAD && kk < 2 * s) break;  // warp-uniform; later stages start later still
         const int n = k - s;  // arriving row (input of sweep s+1)
         float2 ub[2][2];
 #pragma unroll
@@ -177,6 +181,15 @@ __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW 
         rslot = (rslot + 1 == kWideRawSlots) ? 0 : rslot + 1;
         cslot = (cslot + 1 == GeoW<T>::coef_slots) ? 0 : cslot + 1;
     };
+    // A segment starting T or more rows below the top (k0 = y_start - T > 0) needs stage s's
+    // output only from row y_start - (T-1-s) = k0 + s + 1 on, which it first emits at
+    // segment step 2s + 2, from the rows it receives at steps 2s and 2s + 1 (stage s-1's
+    // first valid rows).  Stage s therefore does nothing useful before step 2s: the first
+    // 2T-2 steps skip those stages, T(T-1) stage-steps per segment.
+    if (k0 >= T && k0 + 2 * T - 2 <= khi) {
+        for (int kk = 0; kk < 2 * T - 2; ++kk, advance())
+            stream_step_w<T, XEDGE, false, true>(p, it, w, k, rslot, cslot, kk);
+    }
     if (klo + 1 <= khi) {
         for (; k < klo; advance()) stream_step_w<T, XEDGE, true>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
