@@ -206,9 +206,11 @@ __device__ __forceinline__ void issue_row(const Item &it, int slot, int row, con
 }
 
 // One streaming step: row k arrives at stage 0, stage s emits sweep s+1 of row k-s-1.
-template <int T, bool FAST, bool XEDGE, bool EDGE, bool DUMP>
+// HEAD: one of the first 2T-2 steps of a segment that starts T or more rows below the
+// image top; stage s only runs from its segment step kk = k - k0 = 2s on (see stream_item).
+template <int T, bool FAST, bool XEDGE, bool EDGE, bool DUMP, bool HEAD = false>
 __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it, Win<FAST> (&w)[T][2],
-                                            int k, int rslot, int cslot) {
+                                            int k, int rslot, int cslot, int kk = 0) {
     // Prefetch row k + kPrefetch into the slot row k-1 used, then wait for row k (never
     // beyond the item's last row: rows past it may belong to tiles that a later pass is
     // already rewriting).  A row's chunks are copied by different lanes than the ones
@@ -245,6 +247,7 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
 
 #pragma unroll
     for (int s = 0; s < T; ++s) {
+        if (HEAD && kk < 2 * s) break;  // warp-uniform; later stages start later still
         const int n = k - s;  // arriving row (input of sweep s+1)
         float2 ub[2];
 #pragma unroll
@@ -330,6 +333,18 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
         rslot = (rslot + 1) & (kRawSlots - 1);
         cslot = (cslot + 1 == Geo<T>::coef_slots) ? 0 : cslot + 1;
     };
+    // A segment starting T or more rows below the top (k0 = y_start - T > 0) needs stage s's
+    // output only from row y_start - (T-1-s) = k0 + s + 1 on, which it first emits at
+    // segment step 2s + 2, from the rows it receives at steps 2s and 2s + 1 (stage s-1's
+    // first valid rows).  Stage s therefore does nothing useful before step 2s: the first
+    // 2T-2 steps skip those stages, T(T-1) stage-steps per segment.  (Their rows lie above
+    // y_start, so no dump or store is skipped.)
+    if constexpr (!DUMP) {
+        if (k0 >= T && k0 + 2 * T - 2 <= khi) {
+            for (int kk = 0; kk < 2 * T - 2; ++kk, advance())
+                stream_step<T, FAST, XEDGE, false, DUMP, true>(p, it, w, k, rslot, cslot, kk);
+        }
+    }
     if (klo + 1 <= khi) {
         for (; k < klo; advance()) stream_step<T, FAST, XEDGE, true, DUMP>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
