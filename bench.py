@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--train-sweeps-per-pass", type=int, default=5)
     ap.add_argument("--no-pyramid", action="store_true")
     ap.add_argument("--no-cg", action="store_true")
+    ap.add_argument("--no-exact-form", action="store_true",
+                    help="skip the exact-form leg (its autotuning launches every depth)")
     ap.add_argument("--pyramid-pairs", type=int, default=8)
     return ap.parse_args()
 
@@ -734,7 +736,7 @@ def main():
         # the same step in the exact form (the drop-in's default: the reference program's
         # FP32 operations one rounding at a time, 2 columns per lane, its own tuned depth)
         t_exact = None
-        if not args.exact and not args.shape:
+        if not args.exact and not args.shape and not args.no_exact_form:
             Te, sege, _ = autotune.best_sweep_config(H, W, ld, fast_math=False)
             cfg_e = L.make_config(sweeps_per_pass=Te, rows_per_segment=sege)
 
