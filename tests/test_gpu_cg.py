@@ -17,7 +17,8 @@ def cuda32(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
 
 
-@pytest.mark.parametrize("shape", [(1, 1), (1, 5), (6, 1), (2, 3), (33, 65), (100, 130), (257, 96)])
+@pytest.mark.parametrize("shape", [(1, 1), (1, 5), (6, 1), (2, 3), (33, 65), (100, 130), (257, 96),
+                                   (150, 250), (300, 517)])  # the last two have interior tiles
 @pytest.mark.parametrize("depth", [1, 2, 3, 4])
 def test_matrix_powers_bitexact(cuda, shape, depth):
     H, W = shape
