@@ -69,7 +69,10 @@ __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cas
 
 // HEAD: one of the first 2T-2 steps of a segment that starts T or more rows below the
 // image top; stage s only runs from its segment step kk = k - k0 = 2s on (see stream_item_w).
-template <int T, bool XEDGE, bool EDGE, bool HEAD = false>
+// XE: 0 = no image side in the strip; 1 = a side, any W; 2 = a side with W % 4 == 0, where
+// column W-1 is always a lane's last column (chunks start at multiples of 4), so only the
+// first column's left clamp and the last column's right clamp can apply.
+template <int T, int XE, bool EDGE, bool HEAD = false>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
                                               Win<true> (&w)[T][2][2], int k, int rslot, int cslot,
                                               int kk = 0) {
@@ -111,11 +114,14 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             const float rsh = __shfl_down_sync(kFull, E.x, 1);  // column 4: lane+1's c0
             float2 lE = make_float2(lsh, O.x), rE = O;          // neighbours of (c0, c2)
             float2 rO = make_float2(E.y, rsh);                  // right of (c1, c3); left is E
-            if constexpr (XEDGE) {
+            if constexpr (XE == 1) {
                 lE.x = it.first ? E.x : lE.x;
                 rE.x = (it.last & 1u) ? E.x : rE.x;
                 rO.x = (it.last & 2u) ? O.x : rO.x;
                 rE.y = (it.last & 4u) ? E.y : rE.y;
+                rO.y = (it.last & 8u) ? O.y : rO.y;
+            } else if constexpr (XE == 2) {
+                lE.x = it.first ? E.x : lE.x;
                 rO.y = (it.last & 8u) ? O.y : rO.y;
             }
             ub[q][0] = win_step<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
@@ -157,7 +163,7 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
     }
 }
 
-template <int T, bool XEDGE>
+template <int T, int XE>
 __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
@@ -188,18 +194,18 @@ __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW 
     // 2T-2 steps skip those stages, T(T-1) stage-steps per segment.
     if (k0 >= T && k0 + 2 * T - 2 <= khi) {
         for (int kk = 0; kk < 2 * T - 2; ++kk, advance())
-            stream_step_w<T, XEDGE, false, true>(p, it, w, k, rslot, cslot, kk);
+            stream_step_w<T, XE, false, true>(p, it, w, k, rslot, cslot, kk);
     }
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) stream_step_w<T, XEDGE, true>(p, it, w, k, rslot, cslot);
+        for (; k < klo; advance()) stream_step_w<T, XE, true>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
-            stream_step_w<T, XEDGE, false>(p, it, w, k, rslot, cslot);
+            stream_step_w<T, XE, false>(p, it, w, k, rslot, cslot);
             advance();
-            stream_step_w<T, XEDGE, false>(p, it, w, k, rslot, cslot);
+            stream_step_w<T, XE, false>(p, it, w, k, rslot, cslot);
             advance();
         }
     }
-    for (; k <= k_end; advance()) stream_step_w<T, XEDGE, true>(p, it, w, k, rslot, cslot);
+    for (; k <= k_end; advance()) stream_step_w<T, XE, true>(p, it, w, k, rslot, cslot);
     cp_async_wait<0>();
 }
 
@@ -233,8 +239,12 @@ __device__ __forceinline__ void init_item_w(ItemW &it, const SweepParams &p, int
 template <int T>
 __device__ __forceinline__ void run_item_w(const SweepParams &p, const ItemW &it) {
     const int x0 = it.xa - 4 * it.lane;
-    if (x0 <= 0 || x0 + kWideCols >= p.W) stream_item_w<T, true>(p, it);
-    else stream_item_w<T, false>(p, it);
+    if (x0 <= 0 || x0 + kWideCols >= p.W) {
+        if ((p.W & 3) == 0) stream_item_w<T, 2>(p, it);
+        else stream_item_w<T, 1>(p, it);
+    } else {
+        stream_item_w<T, 0>(p, it);
+    }
 }
 
 int strip_cols_wide(int T);

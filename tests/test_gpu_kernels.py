@@ -174,7 +174,8 @@ def test_misaligned_plane_is_rejected(cuda):
     assert st == L.HS_ERR_ALIGNMENT
 
 
-WIDE_SHAPES = [(1, 1), (1, 5), (67, 1), (1, 67), (3, 5), (2, 200), (130, 257), (257, 130), (64, 128)]
+WIDE_SHAPES = [(1, 1), (1, 5), (67, 1), (1, 67), (3, 5), (2, 200), (130, 257), (257, 130), (64, 128),
+               (97, 256), (33, 500), (50, 4)]  # W % 4 == 0: the side strips' 2-select clamp
 
 
 @pytest.mark.parametrize("shape", WIDE_SHAPES)
