@@ -152,7 +152,14 @@ __device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, f
     acc.w = fmaf(-lr, t, acc.w);
 }
 
-// Global loads one step ahead: the state rows every stage uses at step k.
+__device__ __forceinline__ void prefetch_l2(const float *p) {
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
+// Global loads one step ahead: the state rows every stage uses at step k; and an L2
+// prefetch of the rows of step k + kAdjL2Ahead, so that the register loads find them in L2
+// (the loads' latency was the adjoint's leading stall).
+constexpr int kAdjL2Ahead = 2;
 template <int TB>
 __device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, int k,
                                              float2 (&xs)[TB][2]) {
@@ -162,6 +169,10 @@ __device__ __forceinline__ void adj_prefetch(const AdjPair &P, const Item &it, i
         const size_t off = (size_t)r * P.ld + it.lc2;
         xs[s][0] = __ldg(reinterpret_cast<const float2 *>(P.xu[s] + off));
         xs[s][1] = __ldg(reinterpret_cast<const float2 *>(P.xv[s] + off));
+        const int r2 = min(max(k + kAdjL2Ahead - s, 0), P.H - 1);
+        const size_t off2 = (size_t)r2 * P.ld + it.lc2;
+        prefetch_l2(P.xu[s] + off2);
+        prefetch_l2(P.xv[s] + off2);
     }
 }
 
