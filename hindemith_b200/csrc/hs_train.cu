@@ -129,27 +129,36 @@ template <int TB>
 struct AdjGeo {
     static constexpr int coef_slots = TB + 1;
     static constexpr int raw_floats = Geo<TB>::raw_floats;
-    static constexpr int ring_floats = coef_slots * 2 * 2 * 32 * 4;  // [slot][coef|acc][col][lane] float4
+    static constexpr int ring_floats = coef_slots * 2 * 2 * 32 * 4;  // [slot][4][lane] float4 pairs
     static constexpr int warp_floats = raw_floats + ring_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
 };
 
 // M of one sweep at one column: lambda (lu, lv) -> z, adding this sweep's gradient terms to
-// acc (aIx, aIy, aIt, aA2).  C = (Ix, Iy, It, 1/d); (xu, xv) = x_{k+1}.
+// the accumulators (aIx, aIy, aIt, aA2); (xu, xv) = x_{k+1}, d the denominator.
 // With g = Ix lu + Iy lv, lr = -g/d, t = (Ix xu + Iy xv + It)/alpha^2 and z = lambda + lr (Ix, Iy):
 //   dIx += -lu t + lr ubar + 2 Ix (g t / d) = lr xu - t zu   (ubar = xu + Ix t, g t / d = -lr t)
 //   dIy += lr xv - t zv,   dIt += lr,   dalpha^2 += -lr t
-__device__ __forceinline__ void adj_point(float lu, float lv, const float4 &C, float xu, float xv,
-                                          float inv_a2, float &zu, float &zv, float4 &acc) {
-    const float g = fmaf(C.x, lu, C.y * lv);
-    const float lr = -g * C.w;
-    zu = fmaf(lr, C.x, lu);
-    zv = fmaf(lr, C.y, lv);
-    const float t = fmaf(C.x, xu, fmaf(C.y, xv, C.z)) * inv_a2;
-    acc.x = fmaf(-t, zu, fmaf(lr, xu, acc.x));
-    acc.y = fmaf(-t, zv, fmaf(lr, xv, acc.y));
-    acc.z += lr;
-    acc.w = fmaf(-lr, t, acc.w);
+// The lane's two columns run as packed pairs.  The ring holds, per pair,
+// (Ix, Iy), (It, -1/d), (aIx, aIy) and (aIt, aA2); nia2 = -1/alpha^2.  With the negated
+// factors: lr = g (-1/d), -t = (Ix xu + Iy xv + It)(-1/alpha^2), dIx += lr xu + (-t) zu,
+// dalpha^2 += lr (-t).
+__device__ __forceinline__ void adj_point2(float2 lu, float2 lv, float4 CA, float4 CB, float2 xu,
+                                           float2 xv, float2 nia2, float2 &zu, float2 &zv,
+                                           float4 &AA, float4 &AB) {
+    const float2 cx = make_float2(CA.x, CA.y), cy = make_float2(CA.z, CA.w);
+    const float2 ct = make_float2(CB.x, CB.y), nw = make_float2(CB.z, CB.w);
+    const float2 g = fma2(cx, lu, mul2(cy, lv));
+    const float2 lr = mul2(g, nw);
+    zu = fma2(lr, cx, lu);
+    zv = fma2(lr, cy, lv);
+    const float2 nt = mul2(fma2(cx, xu, fma2(cy, xv, ct)), nia2);
+    const float2 aIx = fma2(nt, zu, fma2(lr, xu, make_float2(AA.x, AA.y)));
+    const float2 aIy = fma2(nt, zv, fma2(lr, xv, make_float2(AA.z, AA.w)));
+    const float2 aIt = add2(make_float2(AB.x, AB.y), lr);
+    const float2 aA = fma2(lr, nt, make_float2(AB.z, AB.w));
+    AA = make_float4(aIx.x, aIx.y, aIy.x, aIy.y);
+    AB = make_float4(aIt.x, aIt.y, aA.x, aA.y);
 }
 
 __device__ __forceinline__ void prefetch_l2(const float *p) {
@@ -190,31 +199,29 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
     constexpr int RW = Geo<TB>::rw;
     const float *raw = it.raw + rslot * (kRawPlanes * RW) + Geo<TB>::sh + 2 * it.lane;
     const float2 l2u = lds2(raw), l2v = lds2(raw + RW);
-    float cu[2][2];
+    float2 cu[2];  // [plane]: the lane's column pair
+    const float2 nia2 = f2(-inv_a2, -inv_a2);
     {
         const float2 ix = lds2(raw + 2 * RW), iy = lds2(raw + 3 * RW);
         const float2 t2 = lds2(raw + 4 * RW);
-        const float ax = rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
-        const float ay = rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
-        const float4 C[2] = {make_float4(ix.x, iy.x, t2.x, ax), make_float4(ix.y, iy.y, t2.y, ay)};
+        const float nax = -rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
+        const float nay = -rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
+        const float4 CA = make_float4(ix.x, ix.y, iy.x, iy.y), CB = make_float4(t2.x, t2.y, nax, nay);
         float4 *slot = ring + cslot * 128 + it.lane;
-        const float lu[2] = {l2u.x, l2u.y}, lv[2] = {l2v.x, l2v.y};
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-            const float xu = j ? xs[0][0].y : xs[0][0].x, xv = j ? xs[0][1].y : xs[0][1].x;
-            adj_point(lu[j], lv[j], C[j], xu, xv, inv_a2, cu[0][j], cu[1][j], acc);
-            slot[32 * j] = C[j];
-            slot[64 + 32 * j] = acc;
-        }
+        float4 AA = make_float4(0.f, 0.f, 0.f, 0.f), AB = AA;
+        adj_point2(l2u, l2v, CA, CB, xs[0][0], xs[0][1], nia2, cu[0], cu[1], AA, AB);
+        slot[0] = CA;
+        slot[32] = CB;
+        slot[64] = AA;
+        slot[96] = AB;
     }
 #pragma unroll
     for (int s = 1; s <= TB; ++s) {
         const int n = k - s + 1;  // arriving row
-        float lam[2][2];
+        float2 lam[2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const float2 c = f2(cu[q][0], cu[q][1]);
+            const float2 c = cu[q];
             const float fromL = __shfl_up_sync(kFull, c.y, 1);
             const float fromR = __shfl_down_sync(kFull, c.x, 1);
             float2 l = f2(fromL, c.x), r = f2(c.y, fromR);
@@ -223,27 +230,19 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
                 r.x = it.a_last ? c.x : r.x;
                 r.y = it.b_last ? c.y : r.y;
             }
-            const float2 m = win_step<EDGE>(w[s - 1][q], l, c, r, n, P.H, f2(we, we), f2(wc, wc));
-            lam[q][0] = m.x;
-            lam[q][1] = m.y;
+            lam[q] = win_step<EDGE>(w[s - 1][q], l, c, r, n, P.H, f2(we, we), f2(wc, wc));
         }
         if (s < TB) {  // M of the next sweep at row k - s
             int rs = cslot - s;
             if (rs < 0) rs += AdjGeo<TB>::coef_slots;
             float4 *slot = ring + rs * 128 + it.lane;
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-                const float4 C = slot[32 * j];
-                float4 acc = slot[64 + 32 * j];
-                const float xu = j ? xs[s][0].y : xs[s][0].x, xv = j ? xs[s][1].y : xs[s][1].x;
-                adj_point(lam[0][j], lam[1][j], C, xu, xv, inv_a2, cu[0][j], cu[1][j], acc);
-                slot[64 + 32 * j] = acc;
-            }
+            float4 AA = slot[64], AB = slot[96];
+            adj_point2(lam[0], lam[1], slot[0], slot[32], xs[s][0], xs[s][1], nia2, cu[0], cu[1], AA, AB);
+            slot[64] = AA;
+            slot[96] = AB;
         } else {
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) cu[q][j] = lam[q][j];
+            cu[0] = lam[0];
+            cu[1] = lam[1];
         }
     }
 
@@ -256,18 +255,18 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
             int rs = cslot - (TB - 1);
             if (rs < 0) rs += AdjGeo<TB>::coef_slots;
             const float4 *slot = ring + rs * 128 + it.lane;
-            const float4 A0 = slot[64], A1 = slot[96];
+            const float4 AA = slot[64], AB = slot[96];  // (aIx, aIy) and (aIt, aA2) pairs
             const size_t off = (size_t)r * P.ld + it.xa;
             if (it.st_a && it.st_b) {
-                atomicAdd(reinterpret_cast<float2 *>(P.aIx + off), make_float2(A0.x, A1.x));
-                atomicAdd(reinterpret_cast<float2 *>(P.aIy + off), make_float2(A0.y, A1.y));
-                atomicAdd(reinterpret_cast<float2 *>(P.aIt + off), make_float2(A0.z, A1.z));
-                a2s += A0.w + A1.w;
+                atomicAdd(reinterpret_cast<float2 *>(P.aIx + off), make_float2(AA.x, AA.y));
+                atomicAdd(reinterpret_cast<float2 *>(P.aIy + off), make_float2(AA.z, AA.w));
+                atomicAdd(reinterpret_cast<float2 *>(P.aIt + off), make_float2(AB.x, AB.y));
+                a2s += AB.z + AB.w;
             } else if (it.st_a) {
-                atomicAdd(P.aIx + off, A0.x);
-                atomicAdd(P.aIy + off, A0.y);
-                atomicAdd(P.aIt + off, A0.z);
-                a2s += A0.w;
+                atomicAdd(P.aIx + off, AA.x);
+                atomicAdd(P.aIy + off, AA.z);
+                atomicAdd(P.aIt + off, AB.x);
+                a2s += AB.z;
             }
         }
     }
@@ -278,11 +277,11 @@ __device__ __forceinline__ void adj_step(const AdjPair &P, const SweepParams &lp
         if (r >= it.y_start && r < it.y_end) {
             const size_t off = (size_t)r * P.ld + it.xa;
             if (it.st_a && it.st_b) {
-                *reinterpret_cast<float2 *>(P.lu_out + off) = make_float2(cu[0][0], cu[0][1]);
-                *reinterpret_cast<float2 *>(P.lv_out + off) = make_float2(cu[1][0], cu[1][1]);
+                *reinterpret_cast<float2 *>(P.lu_out + off) = cu[0];
+                *reinterpret_cast<float2 *>(P.lv_out + off) = cu[1];
             } else if (it.st_a) {
-                P.lu_out[off] = cu[0][0];
-                P.lv_out[off] = cu[1][0];
+                P.lu_out[off] = cu[0].x;
+                P.lv_out[off] = cu[1].x;
             }
         }
     }
