@@ -72,7 +72,8 @@ __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cas
 // XE: 0 = no image side in the strip; 1 = a side, any W; 2 = a side with W % 4 == 0, where
 // column W-1 is always a lane's last column (chunks start at multiples of 4), so only the
 // first column's left clamp and the last column's right clamp can apply.
-template <int T, int XE, bool EDGE, bool HEAD = false>
+// DUMP (the training recompute) also writes every stage's sweep to p.dump_u/v.
+template <int T, int XE, bool EDGE, bool HEAD = false, bool DUMP = false>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
                                               Win<true> (&w)[T][2][2], int k, int rslot, int cslot,
                                               int kk = 0) {
@@ -141,6 +142,25 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             cu[0][j] = fma2(cx, nt, ubar);
             cu[1][j] = fma2(cy, nt, vbar);
         }
+        if constexpr (DUMP) {  // write sweep s+1 of row k-s-1 (state dumps)
+            const int rr = k - s - 1;
+            if (rr >= it.y_start && rr < it.y_end) {
+                const size_t off = (size_t)rr * p.ld + it.xa;
+                const float du[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
+                const float dv[4] = {cu[1][0].x, cu[1][1].x, cu[1][0].y, cu[1][1].y};
+                if (it.st == 15u) {
+                    *reinterpret_cast<float4 *>(p.dump_u[s] + off) = make_float4(du[0], du[1], du[2], du[3]);
+                    *reinterpret_cast<float4 *>(p.dump_v[s] + off) = make_float4(dv[0], dv[1], dv[2], dv[3]);
+                } else if (it.st) {
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (it.st & (1u << j)) {
+                            p.dump_u[s][off + j] = du[j];
+                            p.dump_v[s][off + j] = dv[j];
+                        }
+                }
+            }
+        }
     }
 
     // store sweep T of row k - T
@@ -163,7 +183,7 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
     }
 }
 
-template <int T, int XE>
+template <int T, int XE, bool DUMP>
 __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
@@ -192,20 +212,20 @@ __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW 
     // segment step 2s + 2, from the rows it receives at steps 2s and 2s + 1 (stage s-1's
     // first valid rows).  Stage s therefore does nothing useful before step 2s: the first
     // 2T-2 steps skip those stages, T(T-1) stage-steps per segment.
-    if (k0 >= T && k0 + 2 * T - 2 <= khi) {
+    if (!DUMP && k0 >= T && k0 + 2 * T - 2 <= khi) {  // (dump passes: as the 2-column kernel)
         for (int kk = 0; kk < 2 * T - 2; ++kk, advance())
             stream_step_w<T, XE, false, true>(p, it, w, k, rslot, cslot, kk);
     }
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) stream_step_w<T, XE, true>(p, it, w, k, rslot, cslot);
+        for (; k < klo; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
-            stream_step_w<T, XE, false>(p, it, w, k, rslot, cslot);
+            stream_step_w<T, XE, false, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
-            stream_step_w<T, XE, false>(p, it, w, k, rslot, cslot);
+            stream_step_w<T, XE, false, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
         }
     }
-    for (; k <= k_end; advance()) stream_step_w<T, XE, true>(p, it, w, k, rslot, cslot);
+    for (; k <= k_end; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, k, rslot, cslot);
     cp_async_wait<0>();
 }
 
@@ -236,14 +256,14 @@ __device__ __forceinline__ void init_item_w(ItemW &it, const SweepParams &p, int
     it.alpha2 = p.alpha_dev ? __fmul_rn(__ldg(p.alpha_dev), __ldg(p.alpha_dev)) : p.alpha2;
 }
 
-template <int T>
+template <int T, bool DUMP = false>
 __device__ __forceinline__ void run_item_w(const SweepParams &p, const ItemW &it) {
     const int x0 = it.xa - 4 * it.lane;
     if (x0 <= 0 || x0 + kWideCols >= p.W) {
-        if ((p.W & 3) == 0) stream_item_w<T, 2>(p, it);
-        else stream_item_w<T, 1>(p, it);
+        if ((p.W & 3) == 0) stream_item_w<T, 2, DUMP>(p, it);
+        else stream_item_w<T, 1, DUMP>(p, it);
     } else {
-        stream_item_w<T, 0>(p, it);
+        stream_item_w<T, 0, DUMP>(p, it);
     }
 }
 

@@ -24,7 +24,7 @@
 #include <algorithm>
 #include <vector>
 
-#include "hs_stream.cuh"
+#include "hs_stream4.cuh"
 
 namespace hs {
 
@@ -40,6 +40,7 @@ struct PassTable {
     SweepParams pair[kMaxTrainPairs];
     int item_prefix[kMaxTrainPairs + 1];
     int npairs;
+    bool wide;  // 4 columns per lane (fast form; every pair of the table)
 };
 
 __device__ __forceinline__ int find_pair(const int *prefix, int n, int item) {
@@ -97,7 +98,66 @@ static hs_status launch_table(const PassTable &tab, cudaStream_t s) {
     return HS_OK;
 }
 
+// The same pass in the 4-columns-per-lane layout (fast form only).
+template <int T>
+__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 3 : 2))
+    hs_table_pass_w_kernel(const __grid_constant__ PassTable tab) {
+    extern __shared__ float4 smem4[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *wbase = reinterpret_cast<float *>(smem4) + warp * GeoW<T>::warp_floats;
+    griddep_launch_dependents();
+    griddep_wait();
+    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    if (item >= tab.item_prefix[tab.npairs]) return;
+    const int pi = find_pair(tab.item_prefix, tab.npairs, item);
+    const SweepParams &p = tab.pair[pi];
+    const int local = item - tab.item_prefix[pi];
+    ItemW it;
+    init_item_w<T>(it, p, local % p.nstrips, local / p.nstrips, lane, wbase);
+    if (p.dump) run_item_w<T, true>(p, it);
+    else run_item_w<T, false>(p, it);
+}
+
+template <int T>
+static hs_status launch_table_w(const PassTable &tab, cudaStream_t s) {
+    auto fn = hs_table_pass_w_kernel<T>;
+    static bool attr[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, GeoW<T>::smem_bytes));
+        attr[dev] = true;
+    }
+    const int items = tab.item_prefix[tab.npairs];
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
+    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.dynamicSmemBytes = GeoW<T>::smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, fn, tab));
+    return HS_OK;
+}
+
 static hs_status launch_table_any(int T, bool fast, const PassTable &tab, cudaStream_t s) {
+    if (tab.wide) {
+        switch (T) {
+            case 1: return launch_table_w<1>(tab, s);
+            case 2: return launch_table_w<2>(tab, s);
+            case 3: return launch_table_w<3>(tab, s);
+            case 4: return launch_table_w<4>(tab, s);
+            case 5: return launch_table_w<5>(tab, s);
+            case 6: return launch_table_w<6>(tab, s);
+            case 7: return launch_table_w<7>(tab, s);
+            case 8: return launch_table_w<8>(tab, s);
+        }
+        HS_FAIL(HS_ERR_INVALID_ARG, "pass depth %d outside 1..8", T);
+    }
 #define HS_CASE(TT) \
     case TT: return fast ? launch_table<TT, true>(tab, s) : launch_table<TT, false>(tab, s);
     switch (T) { HS_CASE(1) HS_CASE(2) HS_CASE(3) HS_CASE(4) HS_CASE(5) HS_CASE(6) HS_CASE(7) HS_CASE(8) }
@@ -537,11 +597,26 @@ static SweepParams base_params(const hs_train_pair &d, const float *Ix, const fl
     return p;
 }
 
-// rows per work item for a table launch: about one wave of warps over all pairs
+// The training passes' layout is chosen like the per-pass sweep's, on the pixels of an image
+// (the batch's average): the wide strips pay where images are large (measured: the 8 x 2048^2
+// coarse-to-fine 1 % faster; 16 x 512^2 6 % slower, where 128-column strips cut 512 columns
+// less evenly than 64-column ones).
+static long pair_pixels(const hs_train_pair *pairs, int n) {
+    long px = 0;
+    for (int i = 0; i < n; ++i) px += (long)pairs[i].H * pairs[i].W;
+    return px / std::max(n, 1);
+}
+
+// rows per work item for a table launch: about one wave of warps over all pairs.  In the
+// 4-columns-per-lane layout the strips are re-cut and the wave holds the warps the wide
+// kernel keeps resident (12 per SM to depth 4, 8 beyond).
 static void set_segments(PassTable &tab, int T) {
+    if (tab.wide)
+        for (int i = 0; i < tab.npairs; ++i)
+            tab.pair[i].nstrips = (tab.pair[i].W + strip_cols_wide(T) - 1) / strip_cols_wide(T);
     long rows = 0;
     for (int i = 0; i < tab.npairs; ++i) rows += (long)tab.pair[i].nstrips * tab.pair[i].H;
-    const long target = (long)sm_count() * 16;
+    const long target = (long)sm_count() * (tab.wide ? kWarpsPerBlock * (T <= 4 ? 3 : 2) : 16);
     int L = (int)std::max(1L, (rows + target - 1) / target);
     L = std::max(L, 2 * T);
     tab.item_prefix[0] = 0;
@@ -594,6 +669,7 @@ hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int iters,
         HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.ckpt), 0, 2 * L.pb, s));  // x_0 = 0
     }
     const int T = rc.T;
+    const bool wide = use_wide(rc, pair_pixels(pairs, n));
     for (int b = 0; b < L.nb; ++b) {
         const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
         const int passes = (nsw + T - 1) / T;
@@ -602,6 +678,7 @@ hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int iters,
             PassTable tab;
             memset(&tab, 0, sizeof(tab));
             tab.npairs = n;
+            tab.wide = wide;
             for (int i = 0; i < n; ++i) {
                 SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
                                             plane_at(ws, L, i, 2), rc, t);
@@ -655,6 +732,7 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
     }
     HS_CUDA_CHECK(cudaMemsetAsync(ws + L.partials_off, 0, (size_t)n * L.nslots * sizeof(double), s));
     int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
+    const bool wide = use_wide(rc, pair_pixels(pairs, n));  // the dump passes' layout
     // adjoint depth: at most 4 (a 5-deep adjoint pass is register-bound and slower)
     const int TB = std::min(kAdjMaxDepth, std::max(1, rc.T));
     for (int b = L.nb - 1; b >= 0; --b) {
@@ -665,6 +743,7 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
             PassTable tab;
             memset(&tab, 0, sizeof(tab));
             tab.npairs = n;
+            tab.wide = wide;
             for (int i = 0; i < n; ++i) {
                 SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
                                             plane_at(ws, L, i, 2), rc, t);

@@ -146,12 +146,13 @@ def test_grad_fast_form(cuda):
 
 # ---------------------------------------------------------------- batched training path
 
-def run_batch_grad(imgs, alpha, iters, lams, ckpt_every=10, T=4, fast=True):
+def run_batch_grad(imgs, alpha, iters, lams, ckpt_every=10, T=4, fast=True, layout=0):
     from hindemith_b200.autograd import horn_schunck_batch
 
     a = torch.tensor(alpha, dtype=torch.float32, device="cuda", requires_grad=True)
     xs = [(cuda32(I0).requires_grad_(True), cuda32(I1).requires_grad_(True)) for I0, I1 in imgs]
-    outs = horn_schunck_batch(xs, a, iters, ckpt_every, L.make_config(sweeps_per_pass=T, fast_math=fast))
+    outs = horn_schunck_batch(xs, a, iters, ckpt_every,
+                              L.make_config(sweeps_per_pass=T, fast_math=fast, layout=layout))
     loss = 0
     for (u, v), (lu, lv) in zip(outs, lams):
         loss = loss + (u * cuda32(lu)).sum() + (v * cuda32(lv)).sum()
@@ -178,6 +179,24 @@ def test_batched_grad_matches_fp64_adjoint(cuda, T, ckpt):
         assert rel_err(g0, r0) < REL and rel_err(g1, r1) < REL
         assert np.abs(u - ru).max() < 1e-4
     assert abs(ga - ra_total) <= REL * abs(ra_total)
+
+
+@pytest.mark.parametrize("T", [3, 5])
+def test_batched_grad_wide_layout_identical(cuda, T):
+    """The training passes (forward and dump recompute) in the 4-columns-per-lane layout
+    compute every cell as the 2-column ones: flows and gradients identical bit for bit."""
+    shapes = [(70, 130), (33, 260), (1, 9)]
+    rng = np.random.default_rng(T)
+    imgs = [synthetic.make_pair(H, W, seed=700 + i)[:2] for i, (H, W) in enumerate(shapes)]
+    lams = [(rng.standard_normal(s), rng.standard_normal(s)) for s in shapes]
+    g1, a1, o1 = run_batch_grad(imgs, 0.9, 23, lams, 7, T, layout=1)
+    g2, a2, o2 = run_batch_grad(imgs, 0.9, 23, lams, 7, T, layout=2)
+    for (x0, x1), (y0, y1), (u1, v1), (u2, v2) in zip(g1, g2, o1, o2):
+        assert_bitexact(y0, x0, "dI0")
+        assert_bitexact(y1, x1, "dI1")
+        assert_bitexact(u2, u1, "u")
+        assert_bitexact(v2, v1, "v")
+    assert a1 == a2
 
 
 def test_batched_train_forward_equals_forward(cuda):
