@@ -551,6 +551,9 @@ class Executor:
                 env[name] = val if isinstance(val, DeviceSpMat2D) else DeviceSpMat2D.from_host(val)
             else:
                 env[name] = val
+        args = [v for v in kwargs.values() if isinstance(v, torch.Tensor)]
+        args += [env[n] for n, k in self.prog.params.items() if k == ARRAY2D]
+        handed = {_span(t) for t in args}  # memory the caller holds
         ret = self._block(self.prog.body, env)
         if ret is None:
             return None
@@ -561,7 +564,16 @@ class Executor:
         for n in names:
             v = env[n]
             if isinstance(v, torch.Tensor):
-                v = v.cpu().numpy().copy() if want_numpy else v.clone()
+                if want_numpy:
+                    v = v.cpu().numpy()  # a new host array
+                else:
+                    # values computed by this call are new tensors and are handed out as they
+                    # are; an argument, or a value already handed out, is copied
+                    sp = _span(v)
+                    if any(_overlap(sp, h) for h in handed):
+                        v = v.clone()
+                        sp = _span(v)
+                    handed.add(sp)
             outs.append(v)
         return tuple(outs) if is_tuple else outs[0]
 
@@ -693,6 +705,18 @@ class Executor:
         self.stats["hs_sweeps_calls"] += 1
         env[m["U"]] = u
         env[m["V"]] = v
+
+
+def _span(t) -> tuple:
+    """(device, first byte, one past the last byte) that tensor t may touch."""
+    lo = t.data_ptr()
+    n = sum((d - 1) * st for d, st in zip(t.shape, t.stride())) + 1 if t.numel() else 0
+    return (str(t.device), lo, lo + n * t.element_size())
+
+
+def _overlap(a: tuple, b: tuple) -> bool:
+    """True when two spans of _span share a byte."""
+    return a[0] == b[0] and a[1] < b[2] and b[1] < a[2]
 
 
 def _fdiv(a, b):

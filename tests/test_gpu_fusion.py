@@ -156,3 +156,30 @@ def test_dead_intermediates_stay_in_registers(cuda):
     fused = [s for s in prog.body if s.kind == "Fused"]
     assert len(fused) == 1
     assert set(fused[0].info["outputs"]) == {"w", "u"}  # v is dead after the group
+
+
+def echo_and_repeat(x, y, A2):
+    s = A2 * x
+    t = s + y
+    return x, s, t, s
+
+
+def test_results_never_alias_arguments_or_each_other(cuda, fuse):
+    """Values the call computed come back as they are; an argument, or a value returned twice,
+    comes back as a copy: writing one result changes no argument and no other result."""
+    import torch
+
+    x = torch.from_numpy(rnd((37, 45), 9)).cuda()
+    y = torch.from_numpy(rnd((37, 45), 10)).cuda()
+    x0 = x.clone()
+    got = hm(echo_and_repeat)(x=x, y=y, A2=A)
+    want = np_meaning(echo_and_repeat, x=x0.cpu().numpy(), y=y.cpu().numpy(), A2=A)
+    for g, w in zip(got, want):
+        assert_bitexact(g.cpu().numpy(), w)
+    for g in got:
+        g.fill_(123.0)
+        assert torch.equal(x, x0)
+    for i, g in enumerate(got):
+        g.fill_(float(i))
+        for j, h in enumerate(got[:i]):
+            assert bool((h == float(j)).all()), (i, j)
