@@ -151,12 +151,27 @@ static hs_status compile_fused(const std::string &src, bool fast, Compiled &out)
     return HS_OK;
 }
 
-__global__ void fuse_fold_kernel(const double *partials, int nblocks, int nsums, double *sums) {
-    const int k = threadIdx.x;
-    if (k >= nsums) return;
-    double t = 0.0;
-    for (int b = 0; b < nblocks; ++b) t += partials[(size_t)b * nsums + k];
-    sums[k] = t;
+// Fold of the per-block partials of each sum in a fixed order, the same on every run: thread t
+// adds blocks t, t + kFoldThreads, ... in turn (coalesced across the block), then a
+// shared-memory tree with fixed pairs.  A 1080p grid has 8100 blocks: 8 loads per thread,
+// where a single thread walking them in turn took about 0.25 ms.
+constexpr int kFoldThreads = 1024;
+
+__global__ void __launch_bounds__(kFoldThreads) fuse_fold_kernel(const double *partials, int nblocks,
+                                                                 int nsums, double *sums) {
+    __shared__ double red[kFoldThreads];
+    for (int k = 0; k < nsums; ++k) {
+        double t = 0.0;
+        for (int b = threadIdx.x; b < nblocks; b += kFoldThreads) t += partials[(size_t)b * nsums + k];
+        red[threadIdx.x] = t;
+        __syncthreads();
+        for (int h = kFoldThreads / 2; h > 0; h >>= 1) {
+            if ((int)threadIdx.x < h) red[threadIdx.x] += red[threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) sums[k] = red[0];
+        __syncthreads();  // red[0] is read before the next sum overwrites it
+    }
 }
 
 static inline size_t fuse_blocks(int H, int W) {
@@ -218,8 +233,8 @@ hs_status hs_fused_launch(const char *body, int fast_math, const hs_fused_args *
     HS_CUDA_CHECK(cudaLaunchKernel(reinterpret_cast<const void *>(kern.kernel), grid,
                                    dim3(kFuseBX, kFuseBY), params, 0, s));
     if (args->nsums > 0) {
-        fuse_fold_kernel<<<1, 32, 0, s>>>(partials, (int)fuse_blocks(args->H, args->W), args->nsums,
-                                          args->sums);
+        fuse_fold_kernel<<<1, kFoldThreads, 0, s>>>(partials, (int)fuse_blocks(args->H, args->W),
+                                                    args->nsums, args->sums);
         HS_LAUNCH_CHECK("fuse_fold_kernel");
     }
     return HS_OK;

@@ -43,16 +43,25 @@ __global__ void __launch_bounds__(256) epe_partial_kernel(const __grid_constant_
     }
 }
 
+// Lane i folds pair i's partials in order (the pairs in parallel), then lane 0 adds the pairs'
+// means in order: the same operations, in the same order, as one thread doing both loops.
+static_assert(kEpeMaxPairs <= 32, "one lane per pair");
+
 __global__ void epe_fold_kernel(const __grid_constant__ EpeTable tab, const double *partials,
                                 float *loss) {
-    if (threadIdx.x != 0) return;
-    double total = 0.0;
-    for (int i = 0; i < tab.n; ++i) {
+    __shared__ double mean[kEpeMaxPairs];
+    const int i = threadIdx.x;
+    if (i < tab.n) {
         double s = 0.0;
         for (int b = 0; b < kEpeBlocks; ++b) s += partials[(size_t)i * kEpeBlocks + b];
-        total += s / ((double)tab.pair[i].H * (double)tab.pair[i].W);
+        mean[i] = s / ((double)tab.pair[i].H * (double)tab.pair[i].W);
     }
-    *loss = (float)(total / tab.n);
+    __syncthreads();
+    if (i == 0) {
+        double total = 0.0;
+        for (int j = 0; j < tab.n; ++j) total += mean[j];
+        *loss = (float)(total / tab.n);
+    }
 }
 
 __global__ void __launch_bounds__(256) epe_backward_kernel(const __grid_constant__ EpeTable tab,
