@@ -166,3 +166,25 @@ def f(x, A):
     assert body.count("LD(0,") == 8 and "sqrtf(" in body and "SUM(0," in body and "OUT(0)" in body
     assert gen.inputs == ["x"]
     assert len(gen.scalars) == 2  # the two distinct weights of the average (1/6, 1/12)
+
+
+def test_result_overlap_rule():
+    """The rule that decides which results are copied: two tensors overlap when their byte
+    spans on one device intersect (views of one plane do, neighbouring planes of one
+    allocation do not)."""
+    import torch
+
+    from hindemith_b200.frontend import _overlap, _span
+
+    buf = torch.empty((3, 5, 8), dtype=torch.float32)  # three padded 5 x 7 planes
+    planes = [buf[i, :, :7] for i in range(3)]
+    assert _overlap(_span(planes[0]), _span(planes[0]))
+    assert _overlap(_span(planes[1]), _span(buf[1, 2:4, 3:5]))
+    assert not _overlap(_span(planes[0]), _span(planes[1]))
+    assert not _overlap(_span(planes[1]), _span(planes[2]))
+    assert _overlap(_span(buf), _span(planes[2]))
+    assert not _overlap(_span(torch.empty(0)), _span(planes[0]))
+    other = torch.empty((5, 7))
+    assert not _overlap(_span(other), _span(planes[0]))
+    lo = _span(planes[0])
+    assert not _overlap(("cuda:0",) + lo[1:], lo)  # same addresses on another device
