@@ -18,7 +18,7 @@ from typing import Dict, Tuple
 _cache: Dict[str, Tuple[int, int]] = {}
 _lock = threading.Lock()
 
-T_CANDIDATES = (1, 2, 3, 4, 5, 6, 8)
+T_CANDIDATES = (1, 2, 3, 4, 5, 6, 7, 8)
 
 
 def _seg_candidates(H: int, W: int, T: int):
@@ -99,7 +99,7 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
     for p in planes:
         p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
     Ix, Iy, It, u, v = planes
-    sweeps = 120  # a multiple of every candidate T
+    sweeps = 120  # the same sweep count for every candidate (a partial last pass at T = 7)
     results = []
     for layout in ((1, 2) if fast_math else (1,)):
         for T in candidates:

@@ -122,9 +122,10 @@ def forward_batched(pairs: Sequence[Tuple[torch.Tensor, torch.Tensor, float, int
                     config=None, stream=None) -> List[Tuple[torch.Tensor, torch.Tensor]]:
     """Eager batched forward: [(I0, I1, alpha, iters)] -> [(u, v)] planes."""
     specs = [(int(I0.shape[0]), int(I0.shape[1]), a, n) for I0, I1, a, n in pairs]
-    plan = BatchPlan(specs, config, device=pairs[0][0].device if pairs else None)
-    for i, (I0, I1, _, _) in enumerate(pairs):
-        plan.I0[i].copy_(I0)
-        plan.I1[i].copy_(I1)
-    plan.run(stream)
+    with D.stream_scope(stream):  # planes, copies and the launch all on `stream`
+        plan = BatchPlan(specs, config, device=pairs[0][0].device if pairs else None)
+        for i, (I0, I1, _, _) in enumerate(pairs):
+            plan.I0[i].copy_(I0)
+            plan.I1[i].copy_(I1)
+        plan.run(stream)
     return list(zip(plan.u, plan.v))

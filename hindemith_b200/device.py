@@ -8,7 +8,10 @@ such a layout.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import functools
+import inspect
 from typing import Optional, Tuple
 
 import numpy as np
@@ -20,6 +23,30 @@ from . import _lib as L
 def _require_cuda(t: torch.Tensor, name: str) -> None:
     if not t.is_cuda:
         raise ValueError(f"{name} must be a CUDA tensor (libhsflow has no CPU path)")
+
+
+def on_stream(fn):
+    """Run `fn` with its `stream` argument (when given) as torch's current stream.
+
+    Every tensor the call allocates -- outputs, copied inputs, cached scratch -- then
+    belongs to the stream its kernels run on, so the caching allocator never hands that
+    memory to another stream while those kernels may still use it."""
+    pos = list(inspect.signature(fn).parameters).index("stream")
+
+    @functools.wraps(fn)
+    def wrapper(*args, **kwargs):
+        s = kwargs.get("stream", args[pos] if len(args) > pos else None)
+        if s is None:
+            return fn(*args, **kwargs)
+        with torch.cuda.stream(s):
+            return fn(*args, **kwargs)
+
+    return wrapper
+
+
+def stream_scope(stream=None):
+    """Context making `stream` (when given) torch's current stream."""
+    return contextlib.nullcontext() if stream is None else torch.cuda.stream(stream)
 
 
 def stream_handle(stream: Optional[torch.cuda.Stream] = None) -> ctypes.c_void_p:
@@ -86,13 +113,16 @@ def workspace(nbytes: int, device: torch.device, stream=None) -> torch.Tensor:
     """A cached scratch buffer of at least `nbytes` bytes for (device, stream).
 
     Calls issued on one stream run in order, so they may share its buffer; distinct
-    streams get distinct buffers.
+    streams get distinct buffers.  The buffer is allocated on that stream, so when a
+    larger one replaces it the allocator reuses the old memory only in that stream's
+    order.
     """
     s = stream if stream is not None else torch.cuda.current_stream(device)
     key = (torch.device(device).index, s.cuda_stream)
     buf = _workspaces.get(key)
     if buf is None or buf.numel() < nbytes:
-        buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+        with torch.cuda.stream(s):
+            buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
         _workspaces[key] = buf
     return buf
 
@@ -104,6 +134,7 @@ def release_workspaces() -> None:
 # ------------------------------------------------------------------ operations
 
 
+@on_stream
 def stencil2d(weights, offx, offy, x: torch.Tensor, out: Optional[torch.Tensor] = None,
               stream=None) -> torch.Tensor:
     """out = S * x for the clamp-to-edge stencil S (Stencil2DMVM)."""
@@ -144,6 +175,7 @@ def _same_layout(*ts) -> Tuple[torch.Tensor, ...]:
     return tuple(out)
 
 
+@on_stream
 def array2d_op(op: int, b, c, stream=None) -> torch.Tensor:
     b, c = _same_layout(b, c)
     if b.shape != c.shape:
@@ -155,6 +187,7 @@ def array2d_op(op: int, b, c, stream=None) -> torch.Tensor:
     return a
 
 
+@on_stream
 def array2d_scalar_op(op: int, b, s: float, stream=None) -> torch.Tensor:
     b = as_plane(b)
     a = _like(b)
@@ -164,6 +197,7 @@ def array2d_scalar_op(op: int, b, s: float, stream=None) -> torch.Tensor:
     return a
 
 
+@on_stream
 def scalar_array2d_op(op: int, s: float, b, stream=None) -> torch.Tensor:
     b = as_plane(b)
     a = _like(b)
@@ -173,6 +207,7 @@ def scalar_array2d_op(op: int, s: float, b, stream=None) -> torch.Tensor:
     return a
 
 
+@on_stream
 def array2d_copy(b, stream=None) -> torch.Tensor:
     b = as_plane(b)
     a = _like(b)
@@ -182,6 +217,7 @@ def array2d_copy(b, stream=None) -> torch.Tensor:
     return a
 
 
+@on_stream
 def hs_derivs(I0, I1, stream=None):
     """(Ix, Iy, It) of the 2x2x2 Horn-Schunck derivatives, one fused pass."""
     I0, I1 = _same_layout(I0, I1)
@@ -195,6 +231,7 @@ def hs_derivs(I0, I1, stream=None):
     return Ix, Iy, It
 
 
+@on_stream
 def hs_sweeps(Ix, Iy, It, alpha2: float, iters: int, u: torch.Tensor, v: torch.Tensor,
               config: Optional[L.hs_config] = None, stream=None) -> None:
     """`iters` Jacobi sweeps in place on the planes u, v (same layout as Ix)."""
@@ -212,6 +249,7 @@ def hs_sweeps(Ix, Iy, It, alpha2: float, iters: int, u: torch.Tensor, v: torch.T
                               ctypes.byref(cfg), stream_handle(stream)), "hs_sweeps")
 
 
+@on_stream
 def hs_forward(I0, I1, alpha: float, iters: int, config: Optional[L.hs_config] = None,
                stream=None, out=None):
     """Plain per-pair Horn-Schunck: derivatives, u = v = 0, `iters` sweeps.
@@ -237,6 +275,7 @@ def hs_forward(I0, I1, alpha: float, iters: int, config: Optional[L.hs_config] =
     return u, v
 
 
+@on_stream
 def warp(src, u, v, stream=None) -> torch.Tensor:
     """WarpImg2D: src backward-warped by (u, v) (Operations/OpticalFlow/WarpImg2D.cpp:33-75)."""
     src, u, v = _same_layout(src, u, v)

@@ -387,7 +387,10 @@ HS_API hs_status hs_epe_loss_backward_batched(const hs_epe_pair *pairs, int n, f
  *   - Sizes whose five scratch planes exceed HS_NOALLOC_SCRATCH_BYTES are rejected with
  *     HS_ERR_WORKSPACE before any device work.
  *   - The first call on a device looks up the scratch's device address (with that
- *     device current); make that first call before any stream capture.
+ *     device current); make that first call before any stream capture.  The address
+ *     is kept for the life of the process: after cudaDeviceReset, or after the device's
+ *     primary context is released and created again, the module may load elsewhere, so
+ *     such a caller must not use this entry point on that device any more.
  *   - All calls on a device share the one scratch array and it keeps the last call's
  *     contents (each call initialises what it reads).  Calls that overlap on the GPU --
  *     concurrent streams, or several host threads -- race on it; serialise them.

@@ -8,6 +8,7 @@ from conftest import assert_bitexact
 from hindemith_b200 import _lib as L
 from hindemith_b200 import device as D
 from hindemith_b200 import synthetic
+from hindemith_b200.autotune import BATCH_CANDIDATES
 from hindemith_b200.batched import BatchPlan, forward_batched
 from oracle import hs_oracle as O
 
@@ -110,6 +111,22 @@ def test_batched_wide_layout_equals_per_pair(cuda, T):
     per-pair forward in the 2-column layout, bit for bit."""
     inputs = make_inputs(MIXED)
     plan = run_plan(MIXED, L.make_config(sweeps_per_pass=T, fast_math=True, layout=2), inputs)
+    narrow = L.make_config(sweeps_per_pass=T, fast_math=True, layout=1)
+    for i, ((H, W, alpha, iters), (I0, I1)) in enumerate(zip(MIXED, inputs)):
+        u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()),
+                            D.as_plane(torch.from_numpy(I1).cuda()), alpha, iters, narrow)
+        torch.cuda.synchronize()
+        assert_bitexact(plan.u[i].cpu().numpy(), u.cpu().numpy(), f"u pair {i}")
+        assert_bitexact(plan.v[i].cpu().numpy(), v.cpu().numpy(), f"v pair {i}")
+
+
+@pytest.mark.parametrize("T,rows,layout", BATCH_CANDIDATES)
+def test_batched_every_tuner_candidate_equals_per_pair(cuda, T, rows, layout):
+    """Each (depth, rows per tile, layout) the batch autotuner may pick, in the fast form
+    the benchmark runs: equal to the per-pair forward bit for bit."""
+    inputs = make_inputs(MIXED, 6000)
+    plan = run_plan(MIXED, L.make_config(sweeps_per_pass=T, rows_per_segment=rows,
+                                         fast_math=True, layout=layout), inputs)
     narrow = L.make_config(sweeps_per_pass=T, fast_math=True, layout=1)
     for i, ((H, W, alpha, iters), (I0, I1)) in enumerate(zip(MIXED, inputs)):
         u, v = D.hs_forward(D.as_plane(torch.from_numpy(I0).cuda()),

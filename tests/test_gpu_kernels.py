@@ -16,6 +16,8 @@ from oracle import hs_oracle as O
 pytestmark = pytest.mark.gpu
 
 FAST_TOL = 1e-4
+# Every depth the library accepts (and the autotuner may pick): 1 .. HS_MAX_SWEEPS_PER_PASS.
+ALL_T = list(range(1, L.HS_MAX_SWEEPS_PER_PASS + 1))
 
 
 def dev(a, pad=0):
@@ -72,7 +74,7 @@ def run_sweeps(Ix, Iy, It, alpha2, iters, u0, v0, **cfg):
 
 
 @pytest.mark.parametrize("path", golden_files("hs_*.npz"))
-@pytest.mark.parametrize("T", [1, 2, 3, 4, 5, 8])
+@pytest.mark.parametrize("T", ALL_T)
 def test_sweeps_exact_golden(cuda, path, T):
     d = np.load(path)
     z = np.zeros_like(d["I0"])
@@ -85,7 +87,7 @@ def test_sweeps_exact_golden(cuda, path, T):
 
 @pytest.mark.parametrize("shape", [(1, 1), (1, 2), (1, 67), (67, 1), (2, 2), (3, 5), (5, 3),
                                    (7, 130), (130, 7), (64, 64), (65, 127)])
-@pytest.mark.parametrize("T", [1, 2, 4, 7, 8])
+@pytest.mark.parametrize("T", ALL_T)
 def test_sweeps_exact_edge_shapes(cuda, shape, T):
     H, W = shape
     rng = np.random.default_rng(H * 1000 + W)
@@ -110,13 +112,17 @@ def test_sweeps_pass_parity(cuda, iters):
     assert_bitexact(v, rv, "v")
 
 
-@pytest.mark.parametrize("T", [1, 4, 8])
-def test_sweeps_fast_within_tolerance(cuda, T):
+@pytest.mark.parametrize("T", ALL_T)
+@pytest.mark.parametrize("layout", [1, 2])
+def test_sweeps_fast_within_tolerance(cuda, T, layout):
+    """The fast form at every depth, in both layouts (2 and 4 columns per lane), stays
+    within 1e-4 max-abs of the FP64 oracle."""
     I0, I1, _, _ = synthetic.make_pair(160, 200, seed=1003)
     Ix, Iy, It = O.c_hs_derivs(I0, I1)
     z = np.zeros_like(I0)
     u64, v64 = O.c_hs_sweeps(Ix, Iy, It, 1.0, 200, z, z, np.float64)
-    u, v = run_sweeps(Ix, Iy, It, 1.0, 200, z, z, sweeps_per_pass=T, fast_math=True)
+    u, v = run_sweeps(Ix, Iy, It, 1.0, 200, z, z, sweeps_per_pass=T, fast_math=True,
+                      layout=layout)
     assert np.abs(u - u64).max() < FAST_TOL
     assert np.abs(v - v64).max() < FAST_TOL
 
@@ -166,6 +172,27 @@ def test_nondefault_stream_and_padding(cuda):
     assert_bitexact(v.cpu().numpy(), d["v"], "v")
 
 
+def test_side_stream_with_growing_sizes(cuda):
+    """hs_forward on a side stream, the size growing call by call (so the cached scratch is
+    replaced each time), while the current stream allocates and overwrites memory: every
+    flow equals the same call on the current stream, bit for bit."""
+    s = torch.cuda.Stream()
+    keep, refs, outs = [], [], []
+    for i, (H, W) in enumerate([(64, 96), (200, 300), (400, 610), (700, 1030)]):
+        I0, I1, _, _ = synthetic.make_pair(H, W, seed=700 + i)
+        a, b = dev(I0), dev(I1)
+        keep.append((a, b))
+        refs.append(tuple(host(t) for t in D.hs_forward(a, b, 1.0, 40)))
+        s.wait_stream(torch.cuda.current_stream())
+        outs.append(D.hs_forward(a, b, 1.0, 40, stream=s))
+        junk = torch.full((4 * H * W,), float("nan"), device="cuda")  # reuses freed memory
+        del junk
+    torch.cuda.synchronize()
+    for (u, v), (ru, rv) in zip(outs, refs):
+        assert_bitexact(u.cpu().numpy(), ru, "u")
+        assert_bitexact(v.cpu().numpy(), rv, "v")
+
+
 def test_misaligned_plane_is_rejected(cuda):
     base = torch.zeros((8, 12), device="cuda")
     shifted = base.view(-1)[1:1 + 8 * 8].view(8, 8)  # starts 4 bytes into the buffer
@@ -179,7 +206,7 @@ WIDE_SHAPES = [(1, 1), (1, 5), (67, 1), (1, 67), (3, 5), (2, 200), (130, 257), (
 
 
 @pytest.mark.parametrize("shape", WIDE_SHAPES)
-@pytest.mark.parametrize("T", [1, 3, 4, 5, 8])
+@pytest.mark.parametrize("T", ALL_T)
 def test_wide_layout_equals_narrow(cuda, shape, T):
     """The fast form's 4-columns-per-lane layout computes every cell with the same
     arithmetic as the 2-column one: identical results, bit for bit, at every shape, depth
@@ -207,3 +234,35 @@ def test_wide_layout_full_size(cuda):
     assert_bitexact(got[1], ref[1], "v")
     u64, v64 = O.c_hs_sweeps(Ix, Iy, It, 1.0, 60, z, z, np.float64)
     assert np.abs(got[0] - u64).max() < FAST_TOL and np.abs(got[1] - v64).max() < FAST_TOL
+
+
+def test_autotuner_candidates_are_all_pinned():
+    """Every depth the autotuners may pick is one the parity tests above run."""
+    from hindemith_b200 import autotune
+
+    assert set(autotune.T_CANDIDATES) <= set(ALL_T)
+    assert {c[0] for c in autotune.BATCH_CANDIDATES} <= set(ALL_T)
+
+
+@pytest.mark.parametrize("fast", [True, False])
+def test_plain_1080p_500_at_the_tuned_config(cuda, fast):
+    """The headline workload exactly as the benchmark runs it: 1920x1080, 500 sweeps,
+    alpha 1, at the (depth, segment, layout) the autotuner picks on this device.  The fast
+    form stays within 1e-4 max-abs of the FP64 oracle; the exact form equals the FP32 C
+    oracle bit for bit."""
+    from hindemith_b200 import autotune
+
+    spec = synthetic.plain_1080p()
+    I0, I1, _, _ = synthetic.generate(spec)
+    a, b = dev(I0), dev(I1)
+    T, seg, layout = autotune.best_sweep_config(spec.H, spec.W, D.ld_of(a), fast_math=fast)
+    cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=fast, layout=layout)
+    u, v = (host(t) for t in D.hs_forward(a, b, spec.alpha, spec.iters, cfg))
+    if fast:
+        u64, v64 = O.c_hs_forward(I0, I1, spec.alpha, spec.iters, np.float64)
+        eu, ev = np.abs(u - u64).max(), np.abs(v - v64).max()
+        assert eu < FAST_TOL and ev < FAST_TOL, (T, seg, layout, eu, ev)
+    else:
+        ru, rv = O.c_hs_forward(I0, I1, spec.alpha, spec.iters)
+        assert_bitexact(u, ru, f"u T={T} seg={seg}")
+        assert_bitexact(v, rv, f"v T={T} seg={seg}")
