@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--no-exact-form", action="store_true",
                     help="skip the exact-form leg (its autotuning launches every depth)")
     ap.add_argument("--pyramid-pairs", type=int, default=8)
+    ap.add_argument("--no-hm", action="store_true", help="skip the @hm drop-in leg")
     return ap.parse_args()
 
 
@@ -139,22 +140,149 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-# ------------------------------------------------------------------ CPU baseline
+# ------------------------------------------------------------------ CPU leg
 
-def cpu_baseline(I0, I1, alpha, sweeps):
-    """The reference-kernel restatement (two fused kernels per sweep, FP32, OpenMP over
-    all host cores) on a bounded sample: the full image, `sweeps` sweeps."""
+def c1_sample_rate(O, I0, I1, alpha, sweeps, steps, warm=1):
+    """(Mpix-iters/s, seconds) of `steps` warm calls of the C restatement, each running the
+    derivatives and `sweeps` sweeps of the whole image (the same loop for the CPU baseline
+    and for --impl reference)."""
+    for _ in range(warm):
+        O.c_hs_forward(I0, I1, alpha, sweeps)
+    tot = 0.0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.c_hs_forward(I0, I1, alpha, sweeps)
+        tot += time.perf_counter() - t0
+    H, W = I0.shape
+    return H * W * sweeps * steps / tot / 1e6, tot
+
+
+def cpu_leg_timings(I0, I1, alpha, args):
+    """The CPU baseline: the reference-kernel restatement (two fused kernels per sweep,
+    FP32, OpenMP) timed on the host cores before any GPU work, on bounded samples:
+    the 1080p pair (all cores and 1 thread), the whole 256x256 x100 workload, and the
+    first 8 pairs of the mixed batch at their full sweep counts."""
+    from hindemith_b200 import synthetic
     from oracle import hs_oracle as O
 
     O.lib()
-    O.c_hs_forward(I0[:64, :64], I1[:64, :64], alpha, 2)  # warm the thread pool
-    t0 = time.perf_counter()
-    O.c_hs_forward(I0, I1, alpha, sweeps)
-    dt = time.perf_counter() - t0
+    cores = O.c_num_threads()
+    sweeps = args.cpu_sample_sweeps
+    value, _ = c1_sample_rate(O, I0, I1, alpha, sweeps, args.steps)
     H, W = I0.shape
-    return {"value": H * W * sweeps / dt / 1e6, "unit": UNIT, "cores": O.c_num_threads(),
-            "kind": "port",
-            "sample": f"{W}x{H}, {sweeps} sweeps of the 500-sweep workload, derivatives included"}
+    out = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{W}x{H}, {sweeps} sweeps per step x {args.steps} warm steps (bounded "
+                     f"sample of the 500-sweep workload), derivatives included"}
+    try:
+        O.c_set_num_threads(1)
+        one, _ = c1_sample_rate(O, I0, I1, alpha, 5, 2)
+    finally:
+        O.c_set_num_threads(cores)
+    out["one_thread"] = {"value": one, "unit": UNIT, "cores": 1,
+                         "sample": f"{W}x{H}, 5 sweeps per step x 2 warm steps"}
+    c0 = synthetic.plain_256()
+    a0, b0, _, _ = synthetic.generate(c0)
+    v0, _ = c1_sample_rate(O, a0, b0, c0.alpha, c0.iters, 5)
+    out["c0"] = {"value": v0, "unit": UNIT, "cores": cores,
+                 "sample": "256x256, the whole 100-sweep workload, 5 warm steps"}
+    sub = synthetic.batch_mixed()[:8]
+    pairs = [synthetic.generate(sp) for sp in sub]
+    t = 0.0
+    for (a, b, _, _), sp in zip(pairs, sub):
+        t0 = time.perf_counter()
+        O.c_hs_forward(a, b, sp.alpha, sp.iters)
+        t += time.perf_counter() - t0
+    pix = sum(sp.H * sp.W * sp.iters for sp in sub)
+    out["c2_subset"] = {"value": pix / t / 1e6, "unit": UNIT, "cores": cores,
+                        "sample": f"the first 8 pairs of the 64-pair mixed batch at their full "
+                                  f"sweep counts ({pix / 1e9:.2f} Gpix-it), one pass each; the "
+                                  f"rate per pixel-iteration stands for the whole batch"}
+    return out
+
+
+def _flow_err(u, v, ru, rv):
+    d = float(max(np.abs(u - ru).max(), np.abs(v - rv).max()))
+    scale = float(max(np.abs(ru).max(), np.abs(rv).max(), 1e-30))
+    return {"max_abs": d, "rel": d / scale}
+
+
+def cpu_leg_errors(checks):
+    """The checker half of the CPU leg: each flow the GPU legs computed, against the FP64
+    oracle (errors: max-abs over u and v; rel = max-abs / max |reference flow|).  Gradients
+    against the FP64 reverse-mode oracle and FP64 central differences.  Outside every timed
+    region."""
+    from oracle import hs_oracle as O
+
+    out = {"definition": "max_abs = max |gpu - fp64| over u and v; rel = max_abs / max |fp64 "
+                         "flow|; tolerance 1e-4 max-abs (flows), 1e-3 relative (gradients)"}
+    for name in ("c0", "c1"):
+        if name not in checks:
+            continue
+        c = checks[name]
+        u64, v64 = O.c_hs_forward(c["I0"], c["I1"], c["alpha"], c["iters"], np.float64)
+        e = {"fast": _flow_err(c["fast"][0], c["fast"][1], u64, v64), "fast_config": c["fast_cfg"]}
+        if "exact" in c:
+            ru, rv = O.c_hs_forward(c["I0"], c["I1"], c["alpha"], c["iters"])
+            e["exact"] = _flow_err(c["exact"][0], c["exact"][1], u64, v64)
+            e["exact"]["bit_identical_to_fp32_oracle"] = bool(
+                np.array_equal(c["exact"][0].view(np.uint32), ru.view(np.uint32))
+                and np.array_equal(c["exact"][1].view(np.uint32), rv.view(np.uint32)))
+            e["exact_config"] = c["exact_cfg"]
+        out[name] = e
+    if "c2" in checks:
+        worst, per = None, []
+        for (a, b, alpha, iters), (u, v) in zip(checks["c2"]["pairs"], checks["c2"]["flows"]):
+            u64, v64 = O.c_hs_forward(a, b, alpha, iters, np.float64)
+            e = _flow_err(u, v, u64, v64)
+            per.append(e["max_abs"])
+            if worst is None or e["max_abs"] > worst["max_abs"]:
+                worst = e
+        out["c2"] = {"pairs": len(per), "max_abs_worst_pair": worst["max_abs"],
+                     "rel_worst_pair": worst["rel"], "max_abs_median_pair": float(np.median(per)),
+                     "config": checks["c2"]["cfg"]}
+    if "c3" in checks:
+        out["c3"] = grad_errors(O, checks["c3"])
+    if "c4" in checks:
+        c = checks["c4"]
+        u64, v64 = O.coarse_to_fine_f64(c["I0"], c["I1"], 1.0, c["levels"], c["iters"])
+        out["c4"] = dict(_flow_err(c["flow"][0], c["flow"][1], u64, v64),
+                         sample=c["sample"])
+    return out
+
+
+def grad_errors(O, c):
+    """FP32 gradients of the mean-EPE loss (config 3 settings on a 64x64 crop) against the
+    FP64 reverse-mode oracle, and against FP64 central differences at the 4 pixels of each
+    image with the largest gradient and for alpha."""
+    I0, I1, ut, vt = (np.asarray(x, np.float64) for x in (c["I0"], c["I1"], c["ut"], c["vt"]))
+    iters, alpha = c["iters"], c["alpha"]
+    n = I0.size
+    u, v = O.c_hs_forward(I0, I1, alpha, iters, np.float64)
+    r = np.sqrt((u - ut) ** 2 + (v - vt) ** 2 + 1e-12)
+    r0, r1, ra, _ = O.hs_adjoint_f64(I0, I1, alpha, iters, (u - ut) / (n * r), (v - vt) / (n * r))
+    g0, g1, ga = c["g0"], c["g1"], c["ga"]
+
+    def rel(a, b):
+        return float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+
+    def loss(i0, i1, al):
+        uu, vv = O.c_hs_forward(i0, i1, al, iters, np.float64)
+        return np.sqrt((uu - ut) ** 2 + (vv - vt) ** 2 + 1e-12).mean()
+
+    h, fd_rel = 1e-4, []
+    for g, which in ((g0, 0), (g1, 1)):
+        for flat in np.argsort(-np.abs(g).ravel())[:4]:
+            i, j = divmod(int(flat), g.shape[1])
+            p, m = [I0.copy(), I1.copy()], [I0.copy(), I1.copy()]
+            p[which][i, j] += h
+            m[which][i, j] -= h
+            fd = (loss(*p, alpha) - loss(*m, alpha)) / (2 * h)
+            fd_rel.append(abs(g[i, j] - fd) / abs(fd))
+    fda = (loss(I0, I1, alpha + h) - loss(I0, I1, alpha - h)) / (2 * h)
+    return {"sample": c["sample"],
+            "dI0_rel_vs_fp64_adjoint": rel(g0, r0), "dI1_rel_vs_fp64_adjoint": rel(g1, r1),
+            "dalpha_rel_vs_fp64_adjoint": abs(ga - ra) / abs(ra),
+            "fd_rel_max_8_pixels": float(max(fd_rel)), "dalpha_rel_vs_fd": abs(ga - fda) / abs(fda)}
 
 
 def cpu_baselines_other():
@@ -205,25 +333,19 @@ def run_reference(args, rank, world):
 
     O.lib()
     sweeps = args.cpu_sample_sweeps
-    for _ in range(max(args.warmup, 1) if args.warmup < 3 else 1):
-        O.c_hs_forward(I0, I1, spec.alpha, 2)
-    times = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        O.c_hs_forward(I0, I1, spec.alpha, sweeps)
-        times.append(time.perf_counter() - t0)
-    tot = sum(times)
-    value = spec.H * spec.W * sweeps * args.steps / tot / 1e6
+    value, tot = c1_sample_rate(O, I0, I1, spec.alpha, sweeps, args.steps, warm=max(args.warmup, 1))
     cb = {"value": value, "unit": UNIT, "cores": O.c_num_threads(), "kind": "port",
-          "sample": f"{spec.W}x{spec.H}, {sweeps} sweeps per step (bounded sample of the "
-                    f"{spec.iters}-sweep workload)"}
+          "sample": f"{spec.W}x{spec.H}, {sweeps} sweeps per step x {args.steps} warm steps "
+                    f"(bounded sample of the {spec.iters}-sweep workload), derivatives included"}
     return {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": "hs_plain_1920x1080_500sweeps", "H": spec.H, "W": spec.W,
-                       "iters": spec.iters, "alpha": spec.alpha,
-                       "sample_sweeps_per_step": sweeps},
+                       "iters": spec.iters, "alpha": spec.alpha, "pairs_per_rank": 1,
+                       "parallelism": f"replicas x{world} (rank 0 runs the host cores)",
+                       "l2": "host run: no GPU L2"},
+            "sample_sweeps_per_step": sweeps,
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -252,7 +374,7 @@ def timed_events(fn, k, warmup, flush, stream, label):
     return sum(a.elapsed_time(b) for a, b in evs) / 1e3
 
 
-def measure_batched(args, rank, flush, peak):
+def measure_batched(args, rank, flush, peak, checks=None):
     """The mixed batch (64 pairs, 320x240 .. 2048x2048, alpha in [0.5, 2], 100/200/500
     sweeps): one graph-captured persistent launch, against one plain hs_forward per pair."""
     import torch
@@ -275,10 +397,13 @@ def measure_batched(args, rank, flush, peak):
     cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=rows, fast_math=not args.exact,
                         layout=layout)
     plan = BatchPlan([(sp.H, sp.W, sp.alpha, sp.iters) for sp in specs], cfg)
+    host_pairs = []
     for i, sp in enumerate(specs):
         I0, I1, _, _ = synthetic.generate(sp)
         plan.I0[i].copy_(torch.from_numpy(I0))
         plan.I1[i].copy_(torch.from_numpy(I1))
+        if checks is not None:
+            host_pairs.append((I0, I1, sp.alpha, sp.iters))
     plan.capture()
     stream = torch.cuda.current_stream()
     t_b = timed_events(plan.replay, args.steps, 3, flush, stream, "timed_batched")
@@ -310,6 +435,12 @@ def measure_batched(args, rank, flush, peak):
     same3 = all(torch.equal(plan3.u[i], plan.u[i]) and torch.equal(plan3.v[i], plan.v[i])
                 for i in range(len(specs)))
     del plan3
+    if checks is not None:
+        checks["c2"] = {"pairs": host_pairs,
+                        "flows": [(plan.u[i].cpu().numpy(), plan.v[i].cpu().numpy())
+                                  for i in range(len(specs))],
+                        "cfg": {"sweeps_per_pass": T, "rows_per_tile": rows, "layout": layout,
+                                "fast_math": not args.exact}}
     return {
         "workload": f"hs_batched_{len(specs)}pairs_mixed", "pairs": len(specs),
         "mpix": round(sum(sp.H * sp.W for sp in specs) / 1e6, 3), "pix_iters": px_it,
@@ -331,7 +462,7 @@ def measure_batched(args, rank, flush, peak):
     }
 
 
-def measure_train(args, rank, flush):
+def measure_train(args, rank, flush, checks=None):
     """Differentiable workload: 16 pairs of 512x512, 200 sweeps, alpha learnable (1.0),
     mean end-point error to the synthetic flow, checkpoints every 10 sweeps; the batched
     training API (one launch per pass for all pairs)."""
@@ -368,15 +499,51 @@ def measure_train(args, rank, flush):
     t_f = timed_events(fwd, k, 3, flush, stream, "timed_train_fwd")
     t_fb = timed_events(fwd_bwd, k, 3, flush, stream, "timed_train_fwd_bwd")
     px_it = sum(sp.H * sp.W * sp.iters for sp in specs)
+
+    # the single-pair form (horn_schunck: hs_forward_train + hs_backward) on pair 0
+    from hindemith_b200.autograd import horn_schunck
+
+    def one_fwd():
+        with torch.no_grad():
+            horn_schunck(data[0][0], data[0][1], alpha, 200, 10, cfg)
+
+    def one_fwd_bwd():
+        alpha.grad = None
+        x0 = data[0][0].detach().requires_grad_(True)
+        x1 = data[0][1].detach().requires_grad_(True)
+        u, v = horn_schunck(x0, x1, alpha, 200, 10, cfg)
+        mean_epe_batch([(u, v)], [(data[0][2], data[0][3])]).backward()
+
+    t1f = timed_events(one_fwd, k, 3, flush, stream, "timed_single_fwd")
+    t1fb = timed_events(one_fwd_bwd, k, 3, flush, stream, "timed_single_fwd_bwd")
+    single = {"workload": "one 512x512 pair, 200 sweeps, checkpoints every 10",
+              "api": "horn_schunck (hs_forward_train + hs_backward)",
+              "fwd_ms": t1f / k * 1e3, "fwd_bwd_ms": t1fb / k * 1e3,
+              "fwd_bwd_over_fwd": t1fb / t1f}
+    if checks is not None:
+        # the gradient check: pair 0's top-left 64x64 crop, the same settings and config
+        I0, I1, ut, vt = (a[:64, :64].copy() for a in synthetic.generate(specs[0]))
+        a = torch.tensor(1.0, device="cuda", requires_grad=True)
+        xs = [(D.as_plane(torch.from_numpy(I0).cuda()).requires_grad_(True),
+               D.as_plane(torch.from_numpy(I1).cuda()).requires_grad_(True))]
+        outs = horn_schunck_batch(xs, a, 200, 10, cfg)
+        mean_epe_batch(outs, [(D.as_plane(torch.from_numpy(ut).cuda()),
+                               D.as_plane(torch.from_numpy(vt).cuda()))]).backward()
+        checks["c3"] = {"I0": I0, "I1": I1, "ut": ut, "vt": vt, "iters": 200, "alpha": 1.0,
+                        "g0": xs[0][0].grad.cpu().numpy(), "g1": xs[0][1].grad.cpu().numpy(),
+                        "ga": float(a.grad),
+                        "sample": "pair 0 of the 16x512x512 batch, top-left 64x64 crop, 200 "
+                                  "sweeps, checkpoints every 10, mean EPE, the timed config"}
     return {"workload": "hs_train_16x512x512_200sweeps_ckpt10", "pix_iters": px_it,
             "sweeps_per_pass": T, "api": "horn_schunck_batch (hs_forward_train_batched + hs_backward_batched) + mean_epe_batch",
             "fwd_ms": t_f / k * 1e3, "fwd_bwd_ms": t_fb / k * 1e3,
             "fwd_bwd_over_fwd": t_fb / t_f,
             "fwd_value": px_it * k / t_f / 1e6,
-            "value": px_it * k / t_fb / 1e6, "unit": UNIT + " (forward+backward)"}
+            "value": px_it * k / t_fb / 1e6, "unit": UNIT + " (forward+backward)",
+            "single_pair": single}
 
 
-def measure_pyramid(args, rank, flush):
+def measure_pyramid(args, rank, flush, checks=None):
     """Coarse-to-fine workload: 8 pairs of 2048x2048 with flow up to 12 px, 4 levels
     (binomial blur + decimation), warp of I1 by the upsampled flow at each finer level,
     100 sweeps per level checkpointed every 10, loss = mean end-point error; forward and
@@ -435,6 +602,14 @@ def measure_pyramid(args, rank, flush):
     px_it = sum(sum(((sp.H + (1 << l) - 1) >> l) * ((sp.W + (1 << l) - 1) >> l)
                     for l in range(levels)) * iters for sp in specs)
     del outs, graph
+    if checks is not None:
+        with torch.no_grad():
+            flow = coarse_to_fine([(data[0][0], data[0][1])], alpha0, levels, iters, 10, cfg)[0]
+        checks["c4"] = {"I0": data[0][0].cpu().numpy(), "I1": data[0][1].cpu().numpy(),
+                        "levels": levels, "iters": iters,
+                        "flow": (flow[0].cpu().numpy(), flow[1].cpu().numpy()),
+                        "sample": "pair 0 of the 8x2048x2048 batch, 4 levels x 100 sweeps, "
+                                  "the timed config"}
     return {"workload": f"hs_pyramid_{len(specs)}x2048x2048_4levels_100sweeps_ckpt10",
             "pix_iters_fwd": px_it, "sweeps_per_pass": args.train_sweeps_per_pass,
             "api": "pyramid.coarse_to_fine (hs_blur_down, hs_upsample2, hs_warp, batched HS) "
@@ -523,6 +698,64 @@ def measure_fusion_flow(args, rank, flush, peak):
                    "peak_gbs": peak}
     out["workload"] = ("flow_magnitude_1920x1080 (@hm call end to end, including the host "
                        "read of sum2d; fused vs one operator per statement)")
+    return out
+
+
+def hs_program(I0, I1, Dx, Dy, Dt, A, alpha, u, v):
+    """The Horn-Schunck program as a Hindemith user writes it (integer-literal loop bound,
+    alpha squared by a scalar statement): the drop-in's own workload."""
+    alpha2 = alpha * alpha
+    Ix = Dx * I0 + Dx * I1
+    Iy = Dy * I0 + Dy * I1
+    It = Dt * I1 - Dt * I0
+    den = alpha2 + Ix * Ix + Iy * Iy
+    for i in range(500):
+        ubar = A * u
+        vbar = A * v
+        t = (Ix * ubar + Iy * vbar + It) / den
+        u = ubar - Ix * t
+        v = vbar - Iy * t
+    return u, v
+
+
+def measure_hm(args, rank, flush, I0, I1, I0h, I1h, spec):
+    """The drop-in: the Horn-Schunck program above through @hm at 1920x1080 x500, with no
+    tuning keys in `defines` (the front end autotunes the fused sweep per shape), in the
+    exact form (the default: the reference's FP32 operation order) and the fast form;
+    device-resident torch inputs, and NumPy host inputs (copies in and out included)."""
+    import numpy as np
+    import torch
+
+    from hindemith_b200 import hm, hs_average_stencil, hs_derivative_stencils
+    from hindemith_b200 import hindemith as HM
+
+    stream = torch.cuda.current_stream()
+    f = hm(hs_program)
+    Dx, Dy, Dt = hs_derivative_stencils()
+    A = hs_average_stencil()
+    z = torch.zeros_like(I0)
+    zh = np.zeros_like(I0h)
+    k = max(1, args.steps // 2)
+    px_it = spec.H * spec.W * 500
+    out = {"workload": "hs_program_1920x1080_500sweeps via @hm (keyword arguments, no defines)"}
+    old = dict(HM.defines)
+    try:
+        for form, fast in (("exact", False), ("fast", True)):
+            HM.defines.clear()
+            if fast:
+                HM.defines["hs_fast_math"] = True
+            kw = dict(I0=I0, I1=I1, Dx=Dx, Dy=Dy, Dt=Dt, A=A, alpha=np.float32(spec.alpha),
+                      u=z, v=z)
+            f(**kw)  # compile + autotune (cached per shape)
+            t = timed_events(lambda: f(**kw), k, 3, flush, stream, f"timed_hm_{form}")
+            kwh = dict(kw, I0=I0h, I1=I1h, u=zh, v=zh)
+            th = timed_events(lambda: f(**kwh), k, 1, flush, stream, f"timed_hm_{form}_numpy")
+            out[form] = {"value": px_it * k / t / 1e6, "unit": UNIT, "ms_per_call": t / k * 1e3,
+                         "numpy_in_out": {"value": px_it * k / th / 1e6, "unit": UNIT,
+                                          "ms_per_call": th / k * 1e3}}
+    finally:
+        HM.defines.clear()
+        HM.defines.update(old)
     return out
 
 
@@ -677,6 +910,10 @@ def main():
         workload += f"_{spec.iters}sweeps" if args.shape else ""
     I0h, I1h, _, _ = synthetic.generate(spec)
     H, W, iters, alpha = spec.H, spec.W, spec.iters, spec.alpha
+    cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
+    # the CPU baseline runs first, on an idle host, with the same warm loop as --impl reference
+    cpu_times = cpu_leg_timings(I0h, I1h, alpha, args) if cpu_leg else None
+    checks = {}
     I0 = D.as_plane(torch.from_numpy(I0h).cuda())
     I1 = D.as_plane(torch.from_numpy(I1h).cuda())
     ld = D.ld_of(I0)
@@ -751,6 +988,32 @@ def main():
         # with the L2 flush between steps on the compute stream (counted).
         t_e2e = e2e_pipelined(I0h, I1h, alpha, iters, cfg, args.steps, flush, dist)
     clocks = clk.summary()
+    if cpu_leg:
+        # flows of the timed configurations, for the checker (outside the timed regions)
+        fu, fv = D.hs_forward(I0, I1, alpha, iters, cfg)
+        c1 = {"I0": I0h, "I1": I1h, "alpha": alpha, "iters": iters,
+              "fast": (fu.cpu().numpy(), fv.cpu().numpy()),
+              "fast_cfg": {"sweeps_per_pass": T, "rows_per_segment": seg, "layout": layout,
+                           "fast_math": not args.exact}}
+        if t_exact is not None:
+            eu, ev = D.hs_forward(I0, I1, alpha, iters, cfg_e)
+            c1["exact"] = (eu.cpu().numpy(), ev.cpu().numpy())
+            c1["exact_cfg"] = {"sweeps_per_pass": Te, "rows_per_segment": sege}
+        checks["c1"] = c1
+        if not args.shape:
+            c0 = synthetic.plain_256()
+            a0, b0, _, _ = synthetic.generate(c0)
+            d0, d1 = D.as_plane(torch.from_numpy(a0).cuda()), D.as_plane(torch.from_numpy(b0).cuda())
+            T0, s0, l0 = autotune.best_sweep_config(c0.H, c0.W, D.ld_of(d0), fast_math=True)
+            cf0 = L.make_config(sweeps_per_pass=T0, rows_per_segment=s0, fast_math=True, layout=l0)
+            fu, fv = D.hs_forward(d0, d1, c0.alpha, c0.iters, cf0)
+            eu, ev = D.hs_forward(d0, d1, c0.alpha, c0.iters)  # the library's default config
+            checks["c0"] = {"I0": a0, "I1": b0, "alpha": c0.alpha, "iters": c0.iters,
+                            "fast": (fu.cpu().numpy(), fv.cpu().numpy()),
+                            "fast_cfg": {"sweeps_per_pass": T0, "rows_per_segment": s0,
+                                         "layout": l0, "fast_math": True},
+                            "exact": (eu.cpu().numpy(), ev.cpu().numpy()),
+                            "exact_cfg": "hs_config zeroed (library default)"}
 
     t_step, t_sweeps, t_e2e = max_over_ranks([t_step, t_sweeps, t_e2e])
     if t_exact is not None:
@@ -762,34 +1025,44 @@ def main():
     peak, peak_kind = load_peaks()
     launch_s = t_sweeps / (args.steps * passes)
     achieved = BYTES_PER_PX_PASS * H * W / launch_s / 1e9
-    traffic = None
+    kernel = (f"hs_stream_w_kernel<{T}>" if wide else
+              f"hs_stream_kernel<{T},{'false' if args.exact else 'true'}>")
+    # ncu figures of this very kernel at this shape (profiles/), when one was captured
+    traffic, prof = None, {}
     tpath = os.path.join(HERE, "profiles", "sweep_traffic.json")
     if os.path.exists(tpath):
         with open(tpath) as f:
-            tj = json.load(f)
-        key = f"T{T}_{'exact' if args.exact else 'fast'}"
-        if key in tj:
-            traffic = tj[key]["bytes_per_launch_1080p"]
+            prof = json.load(f)["kernels"].get(f"{kernel}|{W}x{H}", {})
+        traffic = prof.get("dram_bytes")
+    # issue slots the launch used: its warp instructions over the SMSPs' slots in its time
+    sm_mhz = clocks.get("sm_mhz") or 1965.0
+    issue_frac = (prof["inst"] / (launch_s * torch.cuda.get_device_properties(0).multi_processor_count
+                                  * 4 * sm_mhz * 1e6) if "inst" in prof else None)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": warmup, "ms_per_step": t_step / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded blurred noise + sinusoidal flow; see hindemith_b200/synthetic.py)",
-        "config": {"workload": workload, "H": H, "W": W, "iters": iters,
-                   "alpha": alpha, "sweeps_per_pass": T, "rows_per_segment": seg,
-                   "columns_per_lane": 4 if wide else 2,
-                   "fast_math": not args.exact, "pairs_per_rank": 1,
+        "config": {"workload": workload, "H": H, "W": W, "iters": iters, "alpha": alpha,
+                   "pairs_per_rank": 1, "parallelism": f"replicas x{world}",
                    "l2": "flushed between steps (256 MiB write); the 41 MB working set of one "
-                         "pair is L2-resident within a step",
-                   "parallelism": f"replicas x{world}"},
+                         "pair is L2-resident within a step"},
+        "tuning": {"sweeps_per_pass": T, "rows_per_segment": seg,
+                   "columns_per_lane": 4 if wide else 2, "fast_math": not args.exact,
+                   "autotuned": args.sweeps_per_pass == 0},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": (f"hs_stream_w_kernel<{T}>" if wide else
-                                f"hs_stream_kernel<{T},{'false' if args.exact else 'true'}>"),
-                     "peak_source": peak_kind,
+                     "kernel": kernel, "peak_source": peak_kind,
                      "bytes_per_launch": BYTES_PER_PX_PASS * H * W,
-                     "avg_launch_us": launch_s * 1e6},
+                     "avg_launch_us": launch_s * 1e6,
+                     "traffic_source": prof.get("summary"),
+                     "issue_slot_frac": issue_frac,
+                     "note": "at 1920x1080 the pair's 41.5 MB working set is L2-resident within "
+                             "a step: the kernel is issue/latency-bound, so issue_slot_frac (the "
+                             "profiled warp instructions per launch over 4 issue slots x SMs x "
+                             "the sampled SM clock x the live launch time) is its binding "
+                             "fraction"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 2 * H * W * 4,
                 "d2h_bytes_per_step": 2 * H * W * 4, "ms_per_step": t_e2e / args.steps * 1e3,
                 "pipeline": "pinned host -> device -> pinned host every step; copy-in and "
@@ -804,18 +1077,21 @@ def main():
     }
     # the batched and differentiable workloads are single-GPU measurements
     if world == 1 and not args.no_batched and not args.shape:
-        line["batched"] = measure_batched(args, rank, flush, peak)
+        line["batched"] = measure_batched(args, rank, flush, peak, checks if cpu_leg else None)
     if world == 1 and not args.no_train and not args.shape:
-        line["fwd_bwd"] = measure_train(args, rank, flush)
+        line["fwd_bwd"] = measure_train(args, rank, flush, checks if cpu_leg else None)
     if world == 1 and not args.no_cg and not args.shape:
         line["cg"] = measure_cg(args, rank, flush, peak)
         line["fusion_lk_brox"] = measure_fusion_flow(args, rank, flush, peak)
     if world == 1 and not args.no_pyramid and not args.shape:
-        line["pyramid"] = measure_pyramid(args, rank, flush)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(I0h, I1h, alpha, args.cpu_sample_sweeps)
+        line["pyramid"] = measure_pyramid(args, rank, flush, checks if cpu_leg else None)
+    if world == 1 and not args.no_hm and not args.shape:
+        line["hm_dropin"] = measure_hm(args, rank, flush, I0, I1, I0h, I1h, spec)
+    if cpu_leg:
+        line["cpu_baseline"] = cpu_times
         if "cg" in line:
             line["cpu_baseline_other_operators"] = cpu_baselines_other()
+        line["errors_vs_fp64_oracle"] = cpu_leg_errors(checks)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

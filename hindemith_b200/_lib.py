@@ -146,7 +146,8 @@ SIGNATURES = {
     "hs_upsample2": (_i, [_vp, _i, _vp, _i, _i, _i, _f, _vp]),
     "hs_upsample2_adjoint": (_i, [_vp, _i, _i, _i, _vp, _i, _f, _vp]),
     "hs_warp": (_i, [_vp, _vp, _vp, _i, _i, _i, _vp, _vp]),
-    "hs_warp_adjoint": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp]),
+    "hs_warp_adjoint_workspace_bytes": (_sz, [_i, _i, _i]),
+    "hs_warp_adjoint": (_i, [_vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp, _vp, _vp, _sz, _vp]),
     "hs_backward": (_i, [_vp, _i, _i, _i, _vp, _i, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz,
                          _cfgp, _vp]),
 }

@@ -1,19 +1,23 @@
 // hs_batch.cu -- many Horn-Schunck pairs of uneven size in one persistent launch.
 //
 // Work list.  Every (pass, pair, segment, strip) tile of every pair's full T-sweep passes
-// is one work item.  Items are numbered pass-major: all of pass 0 (pair by pair, each
-// pair's tiles segment-major), then pass 1, ...; pairs are sorted by pass count, largest
-// first, so the pairs still active in pass p are a prefix of that order.  Warps take items
-// from a global atomic counter; a warp runs its item with the streaming sweep of
-// hs_stream.cuh and then publishes "tile done through pass p".
+// is one work item; the tiles of one (pair, pass) unit are consecutive, segment-major.
+// Units are ordered by the pair's progress, pass p of a pair with P passes at p / P
+// (ties by pair): a pair of 20 passes contributes a pass wherever a pair of 100 passes has
+// run 5, so the pairs with few passes are spread over the whole launch instead of all
+// finishing early and leaving the longest chains to run alone at the end.  A one-block
+// set-up kernel ranks the units (batch_order_kernel).  Warps take items from a global
+// atomic counter; a warp runs its item with the streaming sweep of hs_stream.cuh and then
+// publishes "tile done through pass p".
 //
 // Dependencies.  A tile's pass p reads rows and columns of pass p-1 reaching at most
 // one tile beyond its own in each direction (the halo is at most T rows and columns, a
 // segment is at least T rows and a strip at least 48 columns), and overwrites the buffer
 // those pass p-1 tiles read.  So pass p of tile (g, s) waits until its 3x3 neighbour
-// tiles have completed pass p-1.  Every tile an item waits on has a smaller item number,
-// so it was taken earlier by a running warp that waits only on smaller numbers still:
-// the waits always end.  Each wait is nevertheless bounded; a wait that gives up records
+// tiles have completed pass p-1.  A pair's pass p-1 unit comes before its pass p unit
+// (p / P grows with p), so every tile an item waits on has a smaller item number; it was
+// taken earlier by a running warp that waits only on smaller numbers still: the waits
+// always end.  Each wait is nevertheless bounded; a wait that gives up records
 // HS_ERR_TIMEOUT in the device status word and raises an abort flag on which every warp
 // stops.  Completion is published with a release store after the tile's writes and the
 // waits use acquire loads; rows are copied with cp.async.cg (L2), so no stale L1 line
@@ -45,17 +49,47 @@ struct BatchPair {
     int nstrips, seg_rows, items;
 };
 
+// Units (pair, pass) ranked by (p * kOrderScale / P, pair): kOrderScale exceeds every
+// pass count, so the keys of one pair's passes are distinct and increasing.
+constexpr long long kOrderScale = 1LL << 30;
+
 struct BatchParams {
-    BatchPair pair[kMaxBatch];  // sorted by `passes`, descending
-    int item_prefix[kMaxBatch + 1];
-    // pass groups: passes [g_p0, g_p1) have the first g_active pairs active
-    int g_p0[kMaxBatch], g_p1[kMaxBatch], g_active[kMaxBatch], g_first[kMaxBatch];
-    int ngroups, npairs, total_items;
+    BatchPair pair[kMaxBatch];
+    int unit_prefix[kMaxBatch + 1];  // units of pairs before pair r (host order)
+    int nunits;                      // all units = unit_prefix[npairs]
+    int *unit_pp;                    // [nunits]: (pass << 8) | pair, in work order
+    int *unit_first;                 // [nunits + 1]: first item of each unit, then the total
+    int npairs, total_items;
     float we, wc;
     unsigned *queue;
     int *status;
     unsigned *abort_flag;
 };
+
+// Rank every unit of the launch and the first item of each (one block).  The rank of unit
+// (r, p) with key K = floor(p S / P_r) is the number of units (j, q) with
+// (floor(q S / P_j), j) < (K, r): for pair j the q with floor(q S / P_j) < K + [j < r], i.e.
+// q < (K + [j < r]) P_j / S, so ceil((K + [j < r]) P_j / S) of them (at most P_j).
+__global__ void __launch_bounds__(1024) batch_order_kernel(const __grid_constant__ BatchParams bp) {
+    for (int u = threadIdx.x; u < bp.nunits; u += blockDim.x) {
+        int r = 0;
+        while (r + 1 < bp.npairs && bp.unit_prefix[r + 1] <= u) ++r;
+        const int p = u - bp.unit_prefix[r];
+        const long long K = (long long)p * kOrderScale / bp.pair[r].passes;
+        long long rank = 0, first = 0;
+        for (int j = 0; j < bp.npairs; ++j) {
+            const long long Pj = bp.pair[j].passes;
+            if (Pj == 0) continue;
+            const long long a = (K + (j < r ? 1 : 0)) * Pj;
+            const long long c = min(Pj, (a + kOrderScale - 1) / kOrderScale);
+            rank += c;
+            first += c * bp.pair[j].items;
+        }
+        bp.unit_pp[rank] = (p << 8) | r;
+        bp.unit_first[rank] = (int)first;
+    }
+    if (threadIdx.x == 0) bp.unit_first[bp.nunits] = bp.total_items;
+}
 
 struct DerivParams {
     const float *I0[kMaxBatch], *I1[kMaxBatch];
@@ -135,22 +169,18 @@ __global__ void wait_selftest_kernel(int *status, unsigned long long max_polls) 
         atomicCAS(status, 0, (int)HS_ERR_TIMEOUT);
 }
 
-// (pass, pair, local tile) of work item `g`.
+// (pass, pair, local tile) of work item `g`: the last unit whose first item is <= g.
 __device__ __forceinline__ void decode(const BatchParams &bp, int g, int &pass, int &pair, int &local) {
-    int j = 0;
-    while (j + 1 < bp.ngroups && g >= bp.g_first[j + 1]) ++j;
-    const int per_pass = bp.item_prefix[bp.g_active[j]];
-    const int r = g - bp.g_first[j];
-    pass = bp.g_p0[j] + r / per_pass;
-    const int t = r % per_pass;
-    int lo = 0, hi = bp.g_active[j] - 1;  // largest i with item_prefix[i] <= t
+    int lo = 0, hi = bp.nunits - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        if (bp.item_prefix[mid] <= t) lo = mid;
+        if (__ldg(bp.unit_first + mid) <= g) lo = mid;
         else hi = mid - 1;
     }
-    pair = lo;
-    local = t - bp.item_prefix[lo];
+    const int pp = __ldg(bp.unit_pp + lo);
+    pass = pp >> 8;
+    pair = pp & 255;
+    local = g - __ldg(bp.unit_first + lo);
 }
 
 template <int T, bool WIDE>
@@ -247,7 +277,8 @@ static int batch_seg_rows(int H, int T, int cfg_rows) {
 }
 
 static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *cfg,
-                            ResolvedConfig &rc, std::vector<PairPlan> &plan, size_t &total) {
+                            ResolvedConfig &rc, std::vector<PairPlan> &plan, size_t &total,
+                            size_t &order_off) {
     hs_status st = resolve_config(cfg, &rc);
     if (st != HS_OK) return st;
     if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
@@ -288,6 +319,14 @@ static hs_status plan_batch(const hs_pair_desc *pairs, int n, const hs_config *c
         p.off_progress = off;
         off += round_up(sizeof(unsigned) * (size_t)p.items, 16);
     }
+    // the unit tables of the two launches (pairs of one layout each): at most one unit per
+    // full pass of every pair, plus one end entry per launch
+    long units = 0;
+    for (const auto &p : plan) units += p.passes;
+    if (units > (1L << 26)) HS_FAIL(HS_ERR_UNSUPPORTED, "batch has %ld passes in all", units);
+    off = round_up(off, 256);
+    order_off = off;
+    off += round_up(sizeof(int) * (size_t)(2 * units + 2), 256);
     total = round_up(off, 256);
     return HS_OK;
 }
@@ -348,8 +387,8 @@ extern "C" {
 size_t hs_forward_batched_workspace_bytes(const hs_pair_desc *pairs, int n, const hs_config *cfg) {
     ResolvedConfig rc;
     std::vector<PairPlan> plan;
-    size_t total = 0;
-    if (plan_batch(pairs, n, cfg, rc, plan, total) != HS_OK) return 0;
+    size_t total = 0, order_off = 0;
+    if (plan_batch(pairs, n, cfg, rc, plan, total, order_off) != HS_OK) return 0;
     return total;
 }
 
@@ -359,8 +398,8 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
     clear_error();
     ResolvedConfig rc;
     std::vector<PairPlan> plan;
-    size_t total = 0;
-    hs_status st = plan_batch(pairs, n, cfg, rc, plan, total);
+    size_t total = 0, order_off = 0;
+    hs_status st = plan_batch(pairs, n, cfg, rc, plan, total, order_off);
     if (st != HS_OK) return st;
     if (!workspace || workspace_bytes < total)
         HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, total);
@@ -437,15 +476,14 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
     }
 
     // persistent kernels over every full pass of every pair: one launch per layout
+    int *order = reinterpret_cast<int *>(ws + order_off);
     for (int lay = 1; lay >= 0; --lay) {
         const bool wide = lay == 1;
-        std::vector<int> order;
+        std::vector<int> members;
         for (int i = 0; i < n; ++i)
-            if (plan[i].wide == wide) order.push_back(i);
-        if (order.empty()) continue;
-        std::stable_sort(order.begin(), order.end(),
-                         [&](int a, int b) { return bpairs[a].passes > bpairs[b].passes; });
-        const int m = (int)order.size();
+            if (plan[i].wide == wide && bpairs[i].passes > 0) members.push_back(i);
+        if (members.empty()) continue;
+        const int m = (int)members.size();
         BatchParams bp;
         memset(&bp, 0, sizeof(bp));
         bp.npairs = m;
@@ -454,31 +492,22 @@ hs_status hs_forward_batched(const hs_pair_desc *pairs, int n, void *workspace,
         bp.queue = reinterpret_cast<unsigned *>(ws + (wide ? 12 : 0));
         bp.status = status;
         bp.abort_flag = abort_flag;
-        bp.item_prefix[0] = 0;
-        for (int r = 0; r < m; ++r) {
-            bp.pair[r] = bpairs[order[r]];
-            bp.item_prefix[r + 1] = bp.item_prefix[r] + bp.pair[r].items;
-        }
-        // pass groups: runs of passes with the same number of active (sorted) pairs
         long total_items = 0;
-        int ng = 0, p0 = 0;
-        for (int r = m; r >= 1; --r) {
-            const int p1 = bp.pair[r - 1].passes;  // the first r pairs are active for p < p1
-            if (p1 > p0) {
-                bp.g_p0[ng] = p0;
-                bp.g_p1[ng] = p1;
-                bp.g_active[ng] = r;
-                bp.g_first[ng] = (int)total_items;
-                total_items += (long)(p1 - p0) * bp.item_prefix[r];
-                ++ng;
-                p0 = p1;
-            }
+        bp.unit_prefix[0] = 0;
+        for (int r = 0; r < m; ++r) {
+            bp.pair[r] = bpairs[members[r]];
+            bp.unit_prefix[r + 1] = bp.unit_prefix[r] + bp.pair[r].passes;
+            total_items += (long)bp.pair[r].passes * bp.pair[r].items;
         }
         if (total_items > 0x7fffffffL) HS_FAIL(HS_ERR_UNSUPPORTED, "batch has too many work items");
-        bp.ngroups = ng;
+        bp.nunits = bp.unit_prefix[m];
         bp.total_items = (int)total_items;
-        if (total_items > 0)
-            if ((st = launch_batch_any(rc.T, rc.fast, wide, bp, s)) != HS_OK) return st;
+        bp.unit_pp = order;
+        bp.unit_first = order + bp.nunits;
+        order += 2 * bp.nunits + 1;
+        batch_order_kernel<<<1, 1024, 0, s>>>(bp);
+        HS_LAUNCH_CHECK("batch_order_kernel");
+        if ((st = launch_batch_any(rc.T, rc.fast, wide, bp, s)) != HS_OK) return st;
     }
 
     // the short last pass of pairs whose sweep count is not a multiple of T

@@ -5,8 +5,10 @@
 // All are one-pass HBM-bound maps.  The adjoints of the blur and of the upsampling are
 // gathers (each output sums the inputs whose forward footprint covers it, clamps folded
 // in), so they are deterministic; the warp's adjoint with respect to the source image
-// scatters along the flow with atomicAdd (float atomics: the summation order, hence the
-// last bits, may vary between runs).
+// scatters along the flow, summed in 64-bit fixed point so that the result does not depend
+// on the order of the atomics (deterministic too).
+#include <algorithm>
+
 #include "hs_common.cuh"
 
 namespace hs {
@@ -159,18 +161,73 @@ __global__ void __launch_bounds__(256) warp_kernel(const float *__restrict__ src
     dst[i] = o;
 }
 
-// Adjoint of warp_kernel given g = dL/ddst: dsrc += (scatter), du, dv (overwritten).
+// Adjoint of warp_kernel given g = dL/ddst.  dL/dsrc is a scatter along the flow (a
+// source pixel collects from every destination pixel whose footprint covers it).  To make
+// the sums independent of the order the atomics land in, every contribution is converted
+// to a 64-bit fixed-point integer with one power-of-two scale per launch and added with
+// integer atomics (integer addition is associative); a last pass converts the sums back.
+//
+// The scale: with m = max |g| < 2^(e+1), a contribution is at most m, and a source pixel
+// collects at most Nmax = min(H W, (2F + 3)^2) contributions, F = max(|u|, |v|) (a source
+// pixel within F + 1 of the destination).  The scale 2^k, k = 61 - (e + 1) - ceil(log2
+// Nmax), keeps every sum below 2^61 in magnitude; each contribution is rounded to a
+// multiple of 2^-k, i.e. to about m 2^-(60 - log2 Nmax) (2^-50 m at F = 12).
+
+// ws[0] = max |g| bits, ws[1] = max(|u|, |v|) bits (non-negative floats order like their
+// bit patterns as unsigned integers)
+__global__ void __launch_bounds__(256) warp_adjoint_scale_kernel(const float *__restrict__ g,
+                                                                 const float *__restrict__ ou,
+                                                                 const float *__restrict__ ov,
+                                                                 int H, int W, int ld,
+                                                                 unsigned *__restrict__ ws) {
+    unsigned mg = 0u, mf = 0u;
+    const long long n = (long long)H * W;
+    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
+         e += (long long)gridDim.x * blockDim.x) {
+        const size_t i = (size_t)(e / W) * ld + (size_t)(e % W);
+        mg = max(mg, __float_as_uint(fabsf(__ldg(g + i))));
+        mf = max(mf, max(__float_as_uint(fabsf(__ldg(ou + i))), __float_as_uint(fabsf(__ldg(ov + i)))));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mg = max(mg, __shfl_xor_sync(0xffffffffu, mg, o));
+        mf = max(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(ws, mg);
+        atomicMax(ws + 1, mf);
+    }
+}
+
+// log2 of the fixed-point scale from the two maxima; false when g or the flow is not finite
+__device__ __forceinline__ bool warp_adjoint_scale(const unsigned *ws, int H, int W, int &k) {
+    const float m = __uint_as_float(ws[0]), F = __uint_as_float(ws[1]);
+    if (!(m <= 3.0e38f) || !(F <= 3.0e38f)) return false;
+    if (m == 0.f) {
+        k = 0;
+        return true;
+    }
+    const double side = 2.0 * ceil((double)F) + 3.0;
+    const double nmax = fmin((double)H * (double)W, side * side);
+    const int hb = (int)ceil(log2(fmax(nmax, 1.0)));
+    k = 61 - (ilogbf(m) + 1) - hb;
+    return true;
+}
+
 __global__ void __launch_bounds__(256) warp_adjoint_kernel(const float *__restrict__ src,
                                                            const float *__restrict__ ou,
                                                            const float *__restrict__ ov,
                                                            const float *__restrict__ g, int H,
                                                            int W, int ld,
-                                                           float *__restrict__ dsrc,
+                                                           const unsigned *__restrict__ scale,
+                                                           unsigned long long *__restrict__ acc,
                                                            float *__restrict__ du,
                                                            float *__restrict__ dv) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
+    int k = 0;
+    const bool finite = warp_adjoint_scale(scale, H, W, k);
     const size_t i = (size_t)y * ld + x;
     const float fx = __ldg(ou + i), fy = __ldg(ov + i), gi = __ldg(g + i);
     const int ix = (int)fx, iy = (int)fy;
@@ -178,21 +235,46 @@ __global__ void __launch_bounds__(256) warp_adjoint_kernel(const float *__restri
     float xf = __fsub_rn(fx, (float)ix), yf = __fsub_rn(fy, (float)iy);
     if (fx < 0.0f) { mx--; xf = (float)__dadd_rn(1.0, (double)xf); }
     if (fy < 0.0f) { my--; yf = (float)__dadd_rn(1.0, (double)yf); }
+    // one contribution w * g as a fixed-point integer (two's complement wraps like the sum)
+    auto add = [&](size_t q, double w) {
+        if (!finite) return;
+        const long long c = __double2ll_rn(scalbn(w * (double)gi, k));
+        atomicAdd(acc + q, (unsigned long long)c);
+    };
     if (x + mx >= 0 && x + mx + 1 < W && y + my >= 0 && y + my + 1 < H) {
         const size_t b = (size_t)(x + mx) + (size_t)(y + my) * ld;
         const float s00 = __ldg(src + b), s10 = __ldg(src + b + 1);
         const float s01 = __ldg(src + b + ld), s11 = __ldg(src + b + ld + 1);
-        atomicAdd(dsrc + b, (1.f - xf) * (1.f - yf) * gi);
-        atomicAdd(dsrc + b + 1, xf * (1.f - yf) * gi);
-        atomicAdd(dsrc + b + ld, (1.f - xf) * yf * gi);
-        atomicAdd(dsrc + b + ld + 1, xf * yf * gi);
+        const double xd = xf, yd = yf, nx = 1.0 - xd, ny = 1.0 - yd;
+        add(b, nx * ny);
+        add(b + 1, xd * ny);
+        add(b + ld, nx * yd);
+        add(b + ld + 1, xd * yd);
         du[i] = gi * fmaf(yf, s11 - s01, (1.f - yf) * (s10 - s00));
         dv[i] = gi * fmaf(xf, s11 - s10, (1.f - xf) * (s01 - s00));
     } else {
-        atomicAdd(dsrc + i, gi);
+        add(i, 1.0);
         du[i] = 0.f;
         dv[i] = 0.f;
     }
+}
+
+// dsrc = the fixed-point sums as floats (one rounding); NaN everywhere when g or the flow
+// held a non-finite value
+__global__ void __launch_bounds__(256) warp_adjoint_fold_kernel(const unsigned *__restrict__ scale,
+                                                                const unsigned long long *__restrict__ acc,
+                                                                int H, int W, int ld,
+                                                                float *__restrict__ dsrc) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= W || y >= H) return;
+    int k = 0;
+    const size_t i = (size_t)y * ld + x;
+    if (!warp_adjoint_scale(scale, H, W, k)) {
+        dsrc[i] = __int_as_float(0x7fc00000);
+        return;
+    }
+    dsrc[i] = (float)scalbn((double)(long long)acc[i], -k);
 }
 
 static inline dim3 g2(int H, int W) { return dim3((unsigned)((W + 63) / 64), (unsigned)((H + 3) / 4)); }
@@ -269,8 +351,15 @@ hs_status hs_warp(const float *src, const float *u, const float *v, int H, int W
     return HS_OK;
 }
 
+size_t hs_warp_adjoint_workspace_bytes(int H, int W, int ld) {
+    (void)W;
+    if (H < 1 || ld < 1) return 0;
+    return 256 + (sizeof(unsigned long long) * (size_t)H * (size_t)ld + 255) / 256 * 256;
+}
+
 hs_status hs_warp_adjoint(const float *src, const float *u, const float *v, const float *ddst,
-                          int H, int W, int ld, float *dsrc, float *du, float *dv, void *stream) {
+                          int H, int W, int ld, float *dsrc, float *du, float *dv,
+                          void *workspace, size_t workspace_bytes, void *stream) {
     clear_error();
     hs_status st = check_plane_geometry(H, W, ld);
     if (st != HS_OK) return st;
@@ -278,8 +367,23 @@ hs_status hs_warp_adjoint(const float *src, const float *u, const float *v, cons
     const char *nm[7] = {"src", "u", "v", "ddst", "dsrc", "du", "dv"};
     for (int k = 0; k < 7; ++k)
         if ((st = check_plane(pl[k], nm[k])) != HS_OK) return st;
-    warp_adjoint_kernel<<<g2(H, W), dim3(64, 4), 0, (cudaStream_t)stream>>>(src, u, v, ddst, H, W, ld, dsrc, du, dv);
+    const size_t need = hs_warp_adjoint_workspace_bytes(H, W, ld);
+    if (!workspace || workspace_bytes < need)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, need);
+    if ((reinterpret_cast<uintptr_t>(workspace) & 255u) != 0)
+        HS_FAIL(HS_ERR_ALIGNMENT, "workspace is not 256-byte aligned");
+    cudaStream_t s = (cudaStream_t)stream;
+    unsigned *scale = reinterpret_cast<unsigned *>(workspace);
+    auto *acc = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(workspace) + 256);
+    HS_CUDA_CHECK(cudaMemsetAsync(workspace, 0, need, s));
+    const long long n = (long long)H * W;
+    const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)sm_count() * 8);
+    warp_adjoint_scale_kernel<<<std::max(blocks, 1), 256, 0, s>>>(ddst, u, v, H, W, ld, scale);
+    HS_LAUNCH_CHECK("warp_adjoint_scale_kernel");
+    warp_adjoint_kernel<<<g2(H, W), dim3(64, 4), 0, s>>>(src, u, v, ddst, H, W, ld, scale, acc, du, dv);
     HS_LAUNCH_CHECK("warp_adjoint_kernel");
+    warp_adjoint_fold_kernel<<<g2(H, W), dim3(64, 4), 0, s>>>(scale, acc, H, W, ld, dsrc);
+    HS_LAUNCH_CHECK("warp_adjoint_fold_kernel");
     return HS_OK;
 }
 

@@ -372,6 +372,7 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
 
 struct ResolvedConfig {
     int T;
+    bool T_default;  // hs_config.sweeps_per_pass was 0: T may follow the image size
     int seg_rows;  // 0 = derive per pass
     bool fast;
     int layout;    // hs_config.layout: 0 automatic, 1 two columns per lane, 2 four
@@ -381,6 +382,8 @@ struct ResolvedConfig {
 // 4-columns-per-lane layout
 bool use_wide(const ResolvedConfig &rc, long pixels);
 hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out);
+// for the per-pair sweep: when no depth was given, the measured default for an H x W image
+void apply_shape_default(ResolvedConfig &rc, int H, int W);
 int strip_cols_for(int T);
 int default_seg_rows(int H, int nstrips, int T);
 hs_status launch_pass(int T, bool fast, const SweepParams &pp, cudaStream_t s);

@@ -22,6 +22,7 @@
 //  3. Transposed derivative stencils and the alpha reduction, per pair.
 // The gradient needs alpha != 0 (t is recovered through 1/alpha^2).
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "hs_stream4.cuh"
@@ -473,7 +474,7 @@ struct FinishTable {
     float *dI0[kMaxTrainPairs], *dI1[kMaxTrainPairs];
     const float *alpha[kMaxTrainPairs];
     float *dalpha[kMaxTrainPairs];
-    const double *a2part;  // [npairs][nslots]
+    const double *a2part[kMaxTrainPairs];  // per pair: nslots partials
     int H[kMaxTrainPairs], W[kMaxTrainPairs], ld[kMaxTrainPairs];
     int npairs;
 };
@@ -516,7 +517,7 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const __grid_constant__
     __shared__ double sh[256];
     const int i = blockIdx.x;
     double s = 0.0;
-    for (int e = threadIdx.x; e < nparts; e += blockDim.x) s += ft.a2part[(size_t)i * nparts + e];
+    for (int e = threadIdx.x; e < nparts; e += blockDim.x) s += ft.a2part[i][e];
     sh[threadIdx.x] = s;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -528,12 +529,38 @@ __global__ void __launch_bounds__(256) batch_fold_kernel(const __grid_constant__
 
 // ------------------------------------------------------------------ host plan
 
+// Where one pair's training buffers live: planes of pb bytes each.
+//   derivs  Ix, Iy, It
+//   ckpt    checkpoint c = x_{c k} (c = 0 .. nb; checkpoint nb is the final state) as (u, v)
+//   states  two buffers (by interval parity) of x_{k_lo + j}, j = 1 .. k-1, as (u, v)
+//   lam     two (lambda_u, lambda_v) buffers
+//   acc     dIx, dIy, dIt accumulators
+//   scratch two (u, v) buffers of the forward's inner passes
+//   a2part  nslots doubles of dL/dalpha^2 partials
+struct PairBufs {
+    char *derivs, *ckpt, *states, *lam, *acc, *scratch;
+    double *a2part;
+    size_t pb;
+    float *at(char *base, size_t i) const { return reinterpret_cast<float *>(base + i * pb); }
+    float *deriv(int q) const { return at(derivs, q); }
+    float *ck(int c, int comp) const { return at(ckpt, 2 * (size_t)c + comp); }
+    int nstate;  // states per buffer (ckpt_every - 1)
+    float *state(int j, int comp, int buf) const {
+        return at(states, 2 * ((size_t)buf * nstate + (size_t)(j - 1)) + comp);
+    }
+    float *lamb(int buf, int comp) const { return at(lam, 2 * (size_t)buf + comp); }
+    float *accum(int q) const { return at(acc, q); }
+    float *scr(int buf, int comp) const { return at(scratch, 2 * (size_t)buf + comp); }
+};
+
+// adjoint work items of one pair in one launch, at most: all rows / rows per item (one wave
+// of warps over the batch) + one partial segment per strip
+static int adj_slots(int maxW) { return sm_count() * kAdjItemsPerSmMax + (maxW + kMinStripCols - 1) / kMinStripCols; }
 
 struct TrainLayout {
     size_t pb;            // plane stride (bytes)
     size_t per_pair;      // bytes per pair
     int nb;               // checkpoint intervals
-    int nstates;          // states kept for one interval (ckpt_every - 1)
     // plane indices inside a pair's block
     size_t derivs, ckpt, states, lam, acc, scratch;
     size_t partials_off;  // after all pairs: [n][nslots] doubles
@@ -541,49 +568,64 @@ struct TrainLayout {
     size_t total;
 };
 
-static hs_status train_layout(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
-                              TrainLayout &L) {
+static hs_status check_train_args(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                                  size_t *pbmax) {
     if (!pairs) HS_FAIL(HS_ERR_INVALID_ARG, "pairs is NULL");
     if (n < 1 || n > kMaxTrainPairs) HS_FAIL(HS_ERR_INVALID_ARG, "n=%d outside 1..%d", n, kMaxTrainPairs);
     if (iters < 1 || ckpt_every < 1)
         HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d must be >= 1", iters, ckpt_every);
-    size_t pbmax = 0;
+    *pbmax = 0;
     for (int i = 0; i < n; ++i) {
         hs_status st = check_plane_geometry(pairs[i].H, pairs[i].W, pairs[i].ld);
         if (st != HS_OK) return st;
         if (pairs[i].reserved != 0) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: reserved must be zero", i);
-        pbmax = std::max(pbmax, round_up(plane_bytes(pairs[i].H, pairs[i].ld), 256));
+        *pbmax = std::max(*pbmax, round_up(plane_bytes(pairs[i].H, pairs[i].ld), 256));
     }
-    L.pb = pbmax;
+    return HS_OK;
+}
+
+static hs_status train_layout(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
+                              TrainLayout &L) {
+    hs_status st = check_train_args(pairs, n, iters, ckpt_every, &L.pb);
+    if (st != HS_OK) return st;
     L.nb = (iters + ckpt_every - 1) / ckpt_every;
-    L.nstates = ckpt_every - 1;
-    L.derivs = 0;                              // 3 planes
-    L.ckpt = 3;                                // (nb + 1) x 2 planes
-    L.states = L.ckpt + 2 * (size_t)(L.nb + 1);  // nstates x 2 planes
-    L.lam = L.states + 2 * (size_t)L.nstates;  // 2 x 2 planes
-    L.acc = L.lam + 4;                         // 3 planes (dIx, dIy, dIt)
-    L.scratch = L.acc + 3;                     // 2 x 2 planes
+    L.derivs = 0;                                    // 3 planes
+    L.ckpt = 3;                                      // (nb + 1) x 2 planes
+    L.states = L.ckpt + 2 * (size_t)(L.nb + 1);      // 2 x (ckpt_every - 1) x 2 planes
+    L.lam = L.states + 4 * (size_t)(ckpt_every - 1); // 2 x 2 planes
+    L.acc = L.lam + 4;                               // 3 planes (dIx, dIy, dIt)
+    L.scratch = L.acc + 3;                           // 2 x 2 planes
     L.per_pair = (L.scratch + 4) * L.pb;
     L.partials_off = (size_t)n * L.per_pair;
-    // items of one pair in one adjoint launch <= (all rows / rows per item) + its strips
     int maxW = 1;
     for (int i = 0; i < n; ++i) maxW = std::max(maxW, pairs[i].W);
-    L.nslots = sm_count() * kAdjItemsPerSmMax + (maxW + kMinStripCols - 1) / kMinStripCols;
+    L.nslots = adj_slots(maxW);
     L.total = L.partials_off + round_up((size_t)n * L.nslots * sizeof(double), 256);
     return HS_OK;
 }
 
-static inline float *plane_at(char *ws, const TrainLayout &L, int i, size_t idx) {
-    return reinterpret_cast<float *>(ws + (size_t)i * L.per_pair + idx * L.pb);
+static PairBufs bufs_in_workspace(char *ws, const TrainLayout &L, int i) {
+    char *b = ws + (size_t)i * L.per_pair;
+    PairBufs B;
+    B.pb = L.pb;
+    B.derivs = b + L.derivs * L.pb;
+    B.ckpt = b + L.ckpt * L.pb;
+    B.states = b + L.states * L.pb;
+    B.lam = b + L.lam * L.pb;
+    B.acc = b + L.acc * L.pb;
+    B.scratch = b + L.scratch * L.pb;
+    B.a2part = reinterpret_cast<double *>(ws + L.partials_off) + (size_t)i * L.nslots;
+    B.nstate = (int)((L.lam - L.states) / 4);
+    return B;
 }
 
-static SweepParams base_params(const hs_train_pair &d, const float *Ix, const float *Iy,
-                               const float *It, const ResolvedConfig &rc, int T) {
+static SweepParams base_params(const hs_train_pair &d, const PairBufs &B, const ResolvedConfig &rc,
+                               int T) {
     SweepParams p;
     memset(&p, 0, sizeof(p));
-    p.Ix = Ix;
-    p.Iy = Iy;
-    p.It = It;
+    p.Ix = B.deriv(0);
+    p.Iy = B.deriv(1);
+    p.It = B.deriv(2);
     p.H = d.H;
     p.W = d.W;
     p.ld = d.ld;
@@ -628,6 +670,258 @@ static void set_segments(PassTable &tab, int T) {
     }
 }
 
+// Forward with checkpoints: derivatives, x_0 = 0, then interval by interval; an interval's
+// first pass reads checkpoint b and its last pass writes checkpoint b + 1.  The final state
+// (checkpoint nb) is copied to the pairs' u, v.
+static hs_status train_forward(const hs_train_pair *pairs, const PairBufs *bufs, int n, int iters,
+                               int ckpt_every, const ResolvedConfig &rc, cudaStream_t s) {
+    hs_status st;
+    for (int i = 0; i < n; ++i) {
+        const hs_train_pair &d = pairs[i];
+        const PairBufs &B = bufs[i];
+        if ((st = hs_derivs(d.I0, d.I1, d.H, d.W, d.ld, B.deriv(0), B.deriv(1), B.deriv(2), s)) != HS_OK)
+            return st;
+        HS_CUDA_CHECK(cudaMemsetAsync(B.ck(0, 0), 0, 2 * B.pb, s));  // x_0 = 0
+    }
+    const int T = rc.T;
+    const bool wide = use_wide(rc, pair_pixels(pairs, n));
+    const int nb = (iters + ckpt_every - 1) / ckpt_every;
+    for (int b = 0; b < nb; ++b) {
+        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
+        const int passes = (nsw + T - 1) / T;
+        for (int q = 0, done = 0; q < passes; ++q) {
+            const int t = std::min(T, nsw - done);
+            PassTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            tab.wide = wide;
+            for (int i = 0; i < n; ++i) {
+                const PairBufs &B = bufs[i];
+                SweepParams p = base_params(pairs[i], B, rc, t);
+                p.u_in = q == 0 ? B.ck(b, 0) : B.scr((q - 1) & 1, 0);
+                p.v_in = q == 0 ? B.ck(b, 1) : B.scr((q - 1) & 1, 1);
+                p.u_out = q == passes - 1 ? B.ck(b + 1, 0) : B.scr(q & 1, 0);
+                p.v_out = q == passes - 1 ? B.ck(b + 1, 1) : B.scr(q & 1, 1);
+                tab.pair[i] = p;
+            }
+            set_segments(tab, t);
+            if ((st = launch_table_any(t, rc.fast, tab, s)) != HS_OK) return st;
+            done += t;
+        }
+    }
+    for (int i = 0; i < n; ++i) {
+        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
+        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].u, bufs[i].ck(nb, 0), pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].v, bufs[i].ck(nb, 1), pl, cudaMemcpyDeviceToDevice, s));
+    }
+    return HS_OK;
+}
+
+// A per-device side stream and events for the backward's two-stream schedule (created on
+// first use outside any stream capture; kept until the process exits).  The mutex is held
+// while a backward enqueues its work, so that calls from several host threads never
+// interleave their records and waits on the shared events.
+struct SideStream {
+    cudaStream_t s = nullptr;
+    cudaEvent_t dump_done[2] = {}, adj_done[2] = {}, start = nullptr;
+};
+static std::mutex g_side_mu;
+static SideStream g_side[64];
+
+static hs_status side_stream(int dev, SideStream **out) {
+    SideStream &S = g_side[dev];
+    if (!S.s) {
+        HS_CUDA_CHECK(cudaStreamCreateWithFlags(&S.s, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; ++i) {
+            HS_CUDA_CHECK(cudaEventCreateWithFlags(&S.dump_done[i], cudaEventDisableTiming));
+            HS_CUDA_CHECK(cudaEventCreateWithFlags(&S.adj_done[i], cudaEventDisableTiming));
+        }
+        HS_CUDA_CHECK(cudaEventCreateWithFlags(&S.start, cudaEventDisableTiming));
+    }
+    *out = &S;
+    return HS_OK;
+}
+
+// Backward of train_forward (the same buffers): per checkpoint interval in reverse, dump
+// passes recompute the interval's states, then adjoint passes of balanced depth reverse its
+// sweeps; last the transposed derivative stencils and the dalpha fold.
+//
+// The recompute of interval b-1 needs only its checkpoint, so it runs on a side stream while
+// the adjoint passes of interval b run on the caller's stream: the two kernels' waves fill
+// each other's tails.  The states are double-buffered by interval parity; the recompute of
+// interval b-1 waits for the adjoint of interval b+1 (the last reader of its buffer), the
+// adjoint of interval b waits for its recompute.  Without a side stream (first use inside a
+// stream capture, or more than 64 devices) the same work runs in order on one stream.
+static hs_status train_backward(const hs_train_pair *pairs, const PairBufs *bufs, int n, int iters,
+                                int ckpt_every, int nslots, const ResolvedConfig &rc,
+                                cudaStream_t s) {
+    hs_status st;
+    for (int i = 0; i < n; ++i) {
+        const PairBufs &B = bufs[i];
+        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
+        HS_CUDA_CHECK(cudaMemcpyAsync(B.lamb(0, 0), pairs[i].dLdu, pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemcpyAsync(B.lamb(0, 1), pairs[i].dLdv, pl, cudaMemcpyDeviceToDevice, s));
+        HS_CUDA_CHECK(cudaMemsetAsync(B.accum(0), 0, 3 * B.pb, s));
+        HS_CUDA_CHECK(cudaMemsetAsync(B.a2part, 0, (size_t)nslots * sizeof(double), s));
+    }
+    int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
+    const bool wide = use_wide(rc, pair_pixels(pairs, n));  // the dump passes' layout
+    // adjoint depth: at most 4 (a 5-deep adjoint pass is register-bound and slower)
+    const int TB = std::min(kAdjMaxDepth, std::max(1, rc.T));
+    const int nb = (iters + ckpt_every - 1) / ckpt_every;
+
+    // 1. states x_{k_lo+1} .. x_{k_lo+nsw-1} of interval b into state buffer b & 1
+    auto dump = [&](int b, cudaStream_t ds) -> hs_status {
+        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
+        const int sb = b & 1;
+        for (int done = 0; done < nsw - 1;) {
+            const int t = std::min(5, nsw - 1 - done);  // dump depth: 9 states = 5 + 4
+            PassTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            tab.wide = wide;
+            for (int i = 0; i < n; ++i) {
+                const PairBufs &B = bufs[i];
+                SweepParams p = base_params(pairs[i], B, rc, t);
+                p.u_in = done == 0 ? B.ck(b, 0) : B.state(done, 0, sb);
+                p.v_in = done == 0 ? B.ck(b, 1) : B.state(done, 1, sb);
+                p.dump = 1;
+                for (int q = 0; q < t; ++q) {
+                    p.dump_u[q] = B.state(done + q + 1, 0, sb);
+                    p.dump_v[q] = B.state(done + q + 1, 1, sb);
+                }
+                p.u_out = p.dump_u[t - 1];
+                p.v_out = p.dump_v[t - 1];
+                tab.pair[i] = p;
+            }
+            set_segments(tab, t);
+            hs_status e = launch_table_any(t, rc.fast, tab, ds);
+            if (e != HS_OK) return e;
+            done += t;
+        }
+        return HS_OK;
+    };
+    // 2. adjoint sweeps j = nsw-1 .. 0 of interval b in ceil(nsw / TB) passes of balanced
+    //    depth (10 = 4 + 3 + 3)
+    auto adjoint = [&](int b) -> hs_status {
+        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
+        const int sb = b & 1;
+        const int npass = (nsw + TB - 1) / TB;
+        for (int jhi = nsw, q = 0; jhi > 0; ++q) {
+            const int tb = (jhi + (npass - q) - 1) / (npass - q);
+            AdjTable tab;
+            memset(&tab, 0, sizeof(tab));
+            tab.npairs = n;
+            tab.we = rc.we;
+            tab.wc = rc.wc;
+            long rows = 0;
+            for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
+            const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
+            int Lr = (int)std::max(1L, (rows + target - 1) / target);
+            Lr = std::max(Lr, std::max(8, 2 * tb));
+            tab.item_prefix[0] = 0;
+            for (int i = 0; i < n; ++i) {
+                const hs_train_pair &d = pairs[i];
+                const PairBufs &B = bufs[i];
+                AdjPair &P = tab.pair[i];
+                P.Ix = B.deriv(0);
+                P.Iy = B.deriv(1);
+                P.It = B.deriv(2);
+                P.lu_in = B.lamb(cur, 0);
+                P.lv_in = B.lamb(cur, 1);
+                P.lu_out = B.lamb(cur ^ 1, 0);
+                P.lv_out = B.lamb(cur ^ 1, 1);
+                for (int qq = 0; qq < tb; ++qq) {
+                    const int j = jhi - qq;  // x_{k_lo + j}
+                    P.xu[qq] = (j == nsw) ? B.ck(b + 1, 0) : B.state(j, 0, sb);
+                    P.xv[qq] = (j == nsw) ? B.ck(b + 1, 1) : B.state(j, 1, sb);
+                }
+                P.aIx = B.accum(0);
+                P.aIy = B.accum(1);
+                P.aIt = B.accum(2);
+                P.a2part = B.a2part;
+                P.alpha_dev = d.alpha;
+                P.H = d.H;
+                P.W = d.W;
+                P.ld = d.ld;
+                P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
+                P.seg_rows = std::min(Lr, d.H);
+                const int items = P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
+                if (items > nslots) HS_FAIL(HS_ERR_INVALID_ARG, "adjoint items %d > slots %d", items, nslots);
+                tab.item_prefix[i + 1] = tab.item_prefix[i] + items;
+            }
+            hs_status e = launch_adj_any(tb, tab, s);
+            if (e != HS_OK) return e;
+            cur ^= 1;
+            jhi -= tb;
+        }
+        return HS_OK;
+    };
+
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    HS_CUDA_CHECK(cudaStreamIsCapturing(s, &cap));
+    std::unique_lock<std::mutex> lock(g_side_mu);
+    SideStream *S = nullptr;
+    if (nb > 1 && dev < 64 && (g_side[dev].s || cap == cudaStreamCaptureStatusNone)) {
+        if ((st = side_stream(dev, &S)) != HS_OK) return st;
+    } else {
+        lock.unlock();
+    }
+    if (!S) {
+        for (int b = nb - 1; b >= 0; --b) {
+            if ((st = dump(b, s)) != HS_OK) return st;
+            if ((st = adjoint(b)) != HS_OK) return st;
+        }
+    } else {
+        // the side stream starts after everything the caller queued before this call
+        HS_CUDA_CHECK(cudaEventRecord(S->start, s));
+        HS_CUDA_CHECK(cudaStreamWaitEvent(S->s, S->start, 0));
+        if ((st = dump(nb - 1, S->s)) != HS_OK) return st;
+        HS_CUDA_CHECK(cudaEventRecord(S->dump_done[(nb - 1) & 1], S->s));
+        for (int b = nb - 1; b >= 0; --b) {
+            if (b >= 1) {  // recompute b-1 into buffer (b-1) & 1, last read by adjoint(b+1)
+                if (b + 1 <= nb - 1) HS_CUDA_CHECK(cudaStreamWaitEvent(S->s, S->adj_done[(b + 1) & 1], 0));
+                if ((st = dump(b - 1, S->s)) != HS_OK) return st;
+            }
+            HS_CUDA_CHECK(cudaStreamWaitEvent(s, S->dump_done[b & 1], 0));
+            if (b >= 1) HS_CUDA_CHECK(cudaEventRecord(S->dump_done[(b - 1) & 1], S->s));
+            if ((st = adjoint(b)) != HS_OK) return st;
+            HS_CUDA_CHECK(cudaEventRecord(S->adj_done[b & 1], s));
+        }
+    }
+
+    // 3. transposed derivative stencils and dalpha
+    FinishTable ft;
+    memset(&ft, 0, sizeof(ft));
+    ft.npairs = n;
+    int maxW = 1, maxH = 1;
+    for (int i = 0; i < n; ++i) {
+        const PairBufs &B = bufs[i];
+        ft.dIx[i] = B.accum(0);
+        ft.dIy[i] = B.accum(1);
+        ft.dIt[i] = B.accum(2);
+        ft.a2part[i] = B.a2part;
+        ft.dI0[i] = pairs[i].dI0;
+        ft.dI1[i] = pairs[i].dI1;
+        ft.alpha[i] = pairs[i].alpha;
+        ft.dalpha[i] = pairs[i].dalpha;
+        ft.H[i] = pairs[i].H;
+        ft.W[i] = pairs[i].W;
+        ft.ld[i] = pairs[i].ld;
+        maxW = std::max(maxW, pairs[i].W);
+        maxH = std::max(maxH, pairs[i].H);
+    }
+    batch_derivs_adjoint_kernel<<<dim3((maxW + 63) / 64, (maxH + 3) / 4, n), dim3(64, 4), 0, s>>>(ft);
+    HS_LAUNCH_CHECK("batch_derivs_adjoint_kernel");
+    batch_fold_kernel<<<n, 256, 0, s>>>(ft, nslots);
+    HS_LAUNCH_CHECK("batch_fold_kernel");
+    return HS_OK;
+}
+
+static size_t plane_stride(int H, int ld) { return round_up(plane_bytes(H, ld), 256); }
+
 }  // namespace hs
 
 using namespace hs;
@@ -660,47 +954,9 @@ hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int iters,
             if ((st = check_plane(pl[q], nm[q])) != HS_OK) return st;
         if (!pairs[i].alpha) HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: alpha (device) is NULL", i);
     }
-    cudaStream_t s = (cudaStream_t)stream;
-    char *ws = reinterpret_cast<char *>(workspace);
-    for (int i = 0; i < n; ++i) {
-        const hs_train_pair &d = pairs[i];
-        float *Ix = plane_at(ws, L, i, 0), *Iy = plane_at(ws, L, i, 1), *It = plane_at(ws, L, i, 2);
-        if ((st = hs_derivs(d.I0, d.I1, d.H, d.W, d.ld, Ix, Iy, It, stream)) != HS_OK) return st;
-        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.ckpt), 0, 2 * L.pb, s));  // x_0 = 0
-    }
-    const int T = rc.T;
-    const bool wide = use_wide(rc, pair_pixels(pairs, n));
-    for (int b = 0; b < L.nb; ++b) {
-        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
-        const int passes = (nsw + T - 1) / T;
-        for (int q = 0, done = 0; q < passes; ++q) {
-            const int t = std::min(T, nsw - done);
-            PassTable tab;
-            memset(&tab, 0, sizeof(tab));
-            tab.npairs = n;
-            tab.wide = wide;
-            for (int i = 0; i < n; ++i) {
-                SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
-                                            plane_at(ws, L, i, 2), rc, t);
-                const size_t in = q == 0 ? L.ckpt + 2 * b : L.scratch + 2 * ((q - 1) & 1);
-                const size_t out = q == passes - 1 ? L.ckpt + 2 * (b + 1) : L.scratch + 2 * (q & 1);
-                p.u_in = plane_at(ws, L, i, in);
-                p.v_in = plane_at(ws, L, i, in + 1);
-                p.u_out = plane_at(ws, L, i, out);
-                p.v_out = plane_at(ws, L, i, out + 1);
-                tab.pair[i] = p;
-            }
-            set_segments(tab, t);
-            if ((st = launch_table_any(t, rc.fast, tab, s)) != HS_OK) return st;
-            done += t;
-        }
-    }
-    for (int i = 0; i < n; ++i) {  // the final state is checkpoint nb; hand it out as (u, v)
-        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
-        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].u, plane_at(ws, L, i, L.ckpt + 2 * L.nb), pl, cudaMemcpyDeviceToDevice, s));
-        HS_CUDA_CHECK(cudaMemcpyAsync(pairs[i].v, plane_at(ws, L, i, L.ckpt + 2 * L.nb + 1), pl, cudaMemcpyDeviceToDevice, s));
-    }
-    return HS_OK;
+    std::vector<PairBufs> bufs(n);
+    for (int i = 0; i < n; ++i) bufs[i] = bufs_in_workspace(reinterpret_cast<char *>(workspace), L, i);
+    return train_forward(pairs, bufs.data(), n, iters, ckpt_every, rc, (cudaStream_t)stream);
 }
 
 hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
@@ -722,123 +978,143 @@ hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int 
         if (!pairs[i].alpha || !pairs[i].dalpha)
             HS_FAIL(HS_ERR_INVALID_ARG, "pair %d: alpha / dalpha (device) NULL", i);
     }
+    std::vector<PairBufs> bufs(n);
+    for (int i = 0; i < n; ++i) bufs[i] = bufs_in_workspace(reinterpret_cast<char *>(workspace), L, i);
+    return train_backward(pairs, bufs.data(), n, iters, ckpt_every, L.nslots, rc, (cudaStream_t)stream);
+}
+
+// ---- the single-pair form: the same passes on caller-held derivative and checkpoint
+// buffers (n = 1)
+
+size_t hs_derivs_bytes(int H, int W, int ld) {
+    (void)W;
+    if (H < 1 || ld < 1) return 0;
+    return 3 * plane_stride(H, ld);
+}
+
+size_t hs_checkpoint_bytes(int H, int W, int ld, int iters, int ckpt_every) {
+    (void)W;
+    if (H < 1 || ld < 1 || iters < 0 || ckpt_every < 1) return 0;
+    if (iters == 0) return 0;
+    const size_t nb = (size_t)((iters + ckpt_every - 1) / ckpt_every);
+    return (nb + 1) * 2 * plane_stride(H, ld);
+}
+
+size_t hs_forward_train_workspace_bytes(int H, int W, int ld) {
+    (void)W;
+    if (H < 1 || ld < 1) return 0;
+    return 4 * plane_stride(H, ld);
+}
+
+size_t hs_backward_workspace_bytes(int H, int W, int ld, int ckpt_every) {
+    if (H < 1 || W < 1 || ld < 1 || ckpt_every < 1) return 0;
+    // states 2 x (ckpt_every - 1) x 2, lambda 2 x 2, accumulators 3 planes, then the partials
+    const size_t planes = 4 * (size_t)(ckpt_every - 1) + 4 + 3;
+    return planes * plane_stride(H, ld) + round_up((size_t)adj_slots(W) * sizeof(double), 256);
+}
+
+hs_status hs_forward_train(const float *I0, const float *I1, int H, int W, int ld,
+                           const float *alpha, int iters, int ckpt_every, float *u, float *v,
+                           float *derivs, float *ckpt, void *workspace, size_t workspace_bytes,
+                           const hs_config *cfg, void *stream) {
+    clear_error();
+    hs_status st = check_plane_geometry(H, W, ld);
+    if (st != HS_OK) return st;
+    const void *planes[5] = {I0, I1, u, v, derivs};
+    const char *names[5] = {"I0", "I1", "u", "v", "derivs"};
+    for (int i = 0; i < 5; ++i)
+        if ((st = check_plane(planes[i], names[i])) != HS_OK) return st;
+    if (!alpha) HS_FAIL(HS_ERR_INVALID_ARG, "alpha (device pointer) is NULL");
+    if (iters < 0 || ckpt_every < 1) HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d", iters, ckpt_every);
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
     cudaStream_t s = (cudaStream_t)stream;
+    const size_t pb = plane_stride(H, ld);
+    if (iters == 0) {  // nothing to checkpoint: the derivatives and u = v = 0
+        char *dv = reinterpret_cast<char *>(derivs);
+        if ((st = hs_derivs(I0, I1, H, W, ld, reinterpret_cast<float *>(dv),
+                            reinterpret_cast<float *>(dv + pb), reinterpret_cast<float *>(dv + 2 * pb),
+                            stream)) != HS_OK)
+            return st;
+        HS_CUDA_CHECK(cudaMemsetAsync(u, 0, plane_bytes(H, ld), s));
+        HS_CUDA_CHECK(cudaMemsetAsync(v, 0, plane_bytes(H, ld), s));
+        return HS_OK;
+    }
+    if ((st = check_plane(ckpt, "ckpt")) != HS_OK) return st;
+    const size_t need = hs_forward_train_workspace_bytes(H, W, ld);
+    if (!workspace || workspace_bytes < need)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, need);
+    if (!aligned16(workspace)) HS_FAIL(HS_ERR_ALIGNMENT, "workspace is not 16-byte aligned");
+    hs_train_pair d;
+    memset(&d, 0, sizeof(d));
+    d.I0 = I0;
+    d.I1 = I1;
+    d.u = u;
+    d.v = v;
+    d.alpha = alpha;
+    d.H = H;
+    d.W = W;
+    d.ld = ld;
+    PairBufs B;
+    memset(&B, 0, sizeof(B));
+    B.pb = pb;
+    B.derivs = reinterpret_cast<char *>(derivs);
+    B.ckpt = reinterpret_cast<char *>(ckpt);
+    B.scratch = reinterpret_cast<char *>(workspace);
+    return train_forward(&d, &B, 1, iters, ckpt_every, rc, s);
+}
+
+hs_status hs_backward(const float *derivs, int H, int W, int ld, const float *alpha, int iters,
+                      int ckpt_every, const float *ckpt, const float *dLdu, const float *dLdv,
+                      float *dI0, float *dI1, float *dalpha, void *workspace,
+                      size_t workspace_bytes, const hs_config *cfg, void *stream) {
+    clear_error();
+    hs_status st = check_plane_geometry(H, W, ld);
+    if (st != HS_OK) return st;
+    const void *planes[6] = {derivs, dLdu, dLdv, dI0, dI1, workspace};
+    const char *names[6] = {"derivs", "dLdu", "dLdv", "dI0", "dI1", "workspace"};
+    for (int i = 0; i < 6; ++i)
+        if ((st = check_plane(planes[i], names[i])) != HS_OK) return st;
+    if (!alpha || !dalpha) HS_FAIL(HS_ERR_INVALID_ARG, "alpha / dalpha (device pointers) NULL");
+    if (iters < 0 || ckpt_every < 1) HS_FAIL(HS_ERR_INVALID_ARG, "iters=%d ckpt_every=%d", iters, ckpt_every);
+    if (iters > 0 && (st = check_plane(ckpt, "ckpt")) != HS_OK) return st;
+    ResolvedConfig rc;
+    if ((st = resolve_config(cfg, &rc)) != HS_OK) return st;
+    const size_t need = hs_backward_workspace_bytes(H, W, ld, ckpt_every);
+    if (workspace_bytes < need)
+        HS_FAIL(HS_ERR_WORKSPACE, "workspace %zu bytes < required %zu", workspace_bytes, need);
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t pb = plane_stride(H, ld);
+    hs_train_pair d;
+    memset(&d, 0, sizeof(d));
+    d.alpha = alpha;
+    d.dLdu = dLdu;
+    d.dLdv = dLdv;
+    d.dI0 = dI0;
+    d.dI1 = dI1;
+    d.dalpha = dalpha;
+    d.H = H;
+    d.W = W;
+    d.ld = ld;
+    if (iters == 0) {  // (u, v) = 0 whatever the images: no gradient reaches them
+        HS_CUDA_CHECK(cudaMemsetAsync(dI0, 0, plane_bytes(H, ld), s));
+        HS_CUDA_CHECK(cudaMemsetAsync(dI1, 0, plane_bytes(H, ld), s));
+        HS_CUDA_CHECK(cudaMemsetAsync(dalpha, 0, sizeof(float), s));
+        return HS_OK;
+    }
     char *ws = reinterpret_cast<char *>(workspace);
-    for (int i = 0; i < n; ++i) {
-        const size_t pl = plane_bytes(pairs[i].H, pairs[i].ld);
-        HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam), pairs[i].dLdu, pl, cudaMemcpyDeviceToDevice, s));
-        HS_CUDA_CHECK(cudaMemcpyAsync(plane_at(ws, L, i, L.lam + 1), pairs[i].dLdv, pl, cudaMemcpyDeviceToDevice, s));
-        HS_CUDA_CHECK(cudaMemsetAsync(plane_at(ws, L, i, L.acc), 0, 3 * L.pb, s));
-    }
-    HS_CUDA_CHECK(cudaMemsetAsync(ws + L.partials_off, 0, (size_t)n * L.nslots * sizeof(double), s));
-    int cur = 0;  // lambda buffer holding dL/dx of the current sweep boundary
-    const bool wide = use_wide(rc, pair_pixels(pairs, n));  // the dump passes' layout
-    // adjoint depth: at most 4 (a 5-deep adjoint pass is register-bound and slower)
-    const int TB = std::min(kAdjMaxDepth, std::max(1, rc.T));
-    for (int b = L.nb - 1; b >= 0; --b) {
-        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
-        // 1. states x_{k_lo+1} .. x_{k_lo+nsw-1} into states[0..nsw-2]
-        for (int done = 0; done < nsw - 1;) {
-            const int t = std::min(5, nsw - 1 - done);  // dump depth: 9 states = 5 + 4
-            PassTable tab;
-            memset(&tab, 0, sizeof(tab));
-            tab.npairs = n;
-            tab.wide = wide;
-            for (int i = 0; i < n; ++i) {
-                SweepParams p = base_params(pairs[i], plane_at(ws, L, i, 0), plane_at(ws, L, i, 1),
-                                            plane_at(ws, L, i, 2), rc, t);
-                const size_t in = done == 0 ? L.ckpt + 2 * b : L.states + 2 * (done - 1);
-                p.u_in = plane_at(ws, L, i, in);
-                p.v_in = plane_at(ws, L, i, in + 1);
-                p.dump = 1;
-                for (int q = 0; q < t; ++q) {
-                    p.dump_u[q] = plane_at(ws, L, i, L.states + 2 * (done + q));
-                    p.dump_v[q] = plane_at(ws, L, i, L.states + 2 * (done + q) + 1);
-                }
-                p.u_out = p.dump_u[t - 1];
-                p.v_out = p.dump_v[t - 1];
-                tab.pair[i] = p;
-            }
-            set_segments(tab, t);
-            if ((st = launch_table_any(t, rc.fast, tab, s)) != HS_OK) return st;
-            done += t;
-        }
-        // 2. adjoint sweeps j = nsw-1 .. 0 in passes of up to TB
-        // the interval's sweeps in ceil(nsw / TB) passes of balanced depth (10 = 4 + 3 + 3)
-        const int npass = (nsw + TB - 1) / TB;
-        for (int jhi = nsw, q = 0; jhi > 0; ++q) {
-            const int tb = (jhi + (npass - q) - 1) / (npass - q);
-            AdjTable tab;
-            memset(&tab, 0, sizeof(tab));
-            tab.npairs = n;
-            tab.we = rc.we;
-            tab.wc = rc.wc;
-            long rows = 0;
-            for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
-            const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
-            int Lr = (int)std::max(1L, (rows + target - 1) / target);
-            Lr = std::max(Lr, std::max(8, 2 * tb));
-            tab.item_prefix[0] = 0;
-            for (int i = 0; i < n; ++i) {
-                const hs_train_pair &d = pairs[i];
-                AdjPair &P = tab.pair[i];
-                P.Ix = plane_at(ws, L, i, 0);
-                P.Iy = plane_at(ws, L, i, 1);
-                P.It = plane_at(ws, L, i, 2);
-                P.lu_in = plane_at(ws, L, i, L.lam + 2 * cur);
-                P.lv_in = plane_at(ws, L, i, L.lam + 2 * cur + 1);
-                P.lu_out = plane_at(ws, L, i, L.lam + 2 * (cur ^ 1));
-                P.lv_out = plane_at(ws, L, i, L.lam + 2 * (cur ^ 1) + 1);
-                for (int q = 0; q < tb; ++q) {
-                    const int j = jhi - q;  // x_{k_lo + j}
-                    const size_t idx = (j == nsw) ? L.ckpt + 2 * (b + 1) : L.states + 2 * (j - 1);
-                    P.xu[q] = plane_at(ws, L, i, idx);
-                    P.xv[q] = plane_at(ws, L, i, idx + 1);
-                }
-                P.aIx = plane_at(ws, L, i, L.acc);
-                P.aIy = plane_at(ws, L, i, L.acc + 1);
-                P.aIt = plane_at(ws, L, i, L.acc + 2);
-                P.a2part = reinterpret_cast<double *>(ws + L.partials_off) + (size_t)i * L.nslots;
-                P.alpha_dev = d.alpha;
-                P.H = d.H;
-                P.W = d.W;
-                P.ld = d.ld;
-                P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
-                P.seg_rows = std::min(Lr, d.H);
-                const int items = P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
-                if (items > L.nslots) HS_FAIL(HS_ERR_INVALID_ARG, "adjoint items %d > slots %d", items, L.nslots);
-                tab.item_prefix[i + 1] = tab.item_prefix[i] + items;
-            }
-            if ((st = launch_adj_any(tb, tab, s)) != HS_OK) return st;
-            cur ^= 1;
-            jhi -= tb;
-        }
-    }
-    // 3. transposed derivative stencils and dalpha
-    FinishTable ft;
-    memset(&ft, 0, sizeof(ft));
-    ft.npairs = n;
-    ft.a2part = reinterpret_cast<const double *>(ws + L.partials_off);
-    int maxW = 1, maxH = 1;
-    for (int i = 0; i < n; ++i) {
-        ft.dIx[i] = plane_at(ws, L, i, L.acc);
-        ft.dIy[i] = plane_at(ws, L, i, L.acc + 1);
-        ft.dIt[i] = plane_at(ws, L, i, L.acc + 2);
-        ft.dI0[i] = pairs[i].dI0;
-        ft.dI1[i] = pairs[i].dI1;
-        ft.alpha[i] = pairs[i].alpha;
-        ft.dalpha[i] = pairs[i].dalpha;
-        ft.H[i] = pairs[i].H;
-        ft.W[i] = pairs[i].W;
-        ft.ld[i] = pairs[i].ld;
-        maxW = std::max(maxW, pairs[i].W);
-        maxH = std::max(maxH, pairs[i].H);
-    }
-    batch_derivs_adjoint_kernel<<<dim3((maxW + 63) / 64, (maxH + 3) / 4, n), dim3(64, 4), 0, s>>>(ft);
-    HS_LAUNCH_CHECK("batch_derivs_adjoint_kernel");
-    batch_fold_kernel<<<n, 256, 0, s>>>(ft, L.nslots);
-    HS_LAUNCH_CHECK("batch_fold_kernel");
-    return HS_OK;
+    const size_t nst = 4 * (size_t)(ckpt_every - 1);
+    PairBufs B;
+    memset(&B, 0, sizeof(B));
+    B.pb = pb;
+    B.derivs = const_cast<char *>(reinterpret_cast<const char *>(derivs));
+    B.ckpt = const_cast<char *>(reinterpret_cast<const char *>(ckpt));
+    B.states = ws;
+    B.lam = ws + nst * pb;
+    B.acc = ws + (nst + 4) * pb;
+    B.a2part = reinterpret_cast<double *>(ws + (nst + 7) * pb);
+    B.nstate = ckpt_every - 1;
+    return train_backward(&d, &B, 1, iters, ckpt_every, adj_slots(W), rc, s);
 }
 
 }  // extern "C"

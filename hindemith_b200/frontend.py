@@ -525,6 +525,7 @@ class Executor:
         self.prog = prog
         self.defines = dict(defines)
         self.stats = {"hs_sweeps_calls": 0, "unfused_loops": 0, "fused_launches": 0}
+        self.last_sweep_config = None  # (depth, rows per segment, layout, fast) of the last HS loop
         if self.defines.get("hs_fuse", True):
             fuse_program(self.prog)
 
@@ -699,10 +700,22 @@ class Executor:
         u = _fresh_copy(env[m["U"]], Ix)
         v = _fresh_copy(env[m["V"]], Ix)
         cfg = self.config()
+        if cfg.sweeps_per_pass == 0 and self.defines.get("hs_autotune", True):
+            # no depth in `defines`: the fastest (depth, segment, layout) for this shape and
+            # form on this device, timed once per process and cached (autotune.py)
+            from .autotune import best_sweep_config
+
+            T, seg, layout = best_sweep_config(Ix.shape[0], Ix.shape[1], Ix.stride(0),
+                                               fast_math=bool(cfg.fast_math))
+            cfg.sweeps_per_pass, cfg.layout = T, layout
+            if cfg.rows_per_segment == 0:
+                cfg.rows_per_segment = seg
         cfg.avg_edge = float(we)
         cfg.avg_corner = float(wc)
         device.hs_sweeps(Ix, Iy, It, np.float32(env[m["alpha2"]]), iters, u, v, cfg)
         self.stats["hs_sweeps_calls"] += 1
+        self.last_sweep_config = (cfg.sweeps_per_pass, cfg.rows_per_segment, cfg.layout,
+                                  bool(cfg.fast_math))
         env[m["U"]] = u
         env[m["V"]] = v
 

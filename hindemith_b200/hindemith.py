@@ -23,9 +23,12 @@ import numpy as np
 from .frontend import Executor, HMCompileError, function_source, parse, symbol_kind
 
 # Module-global tuning constants, as in the reference (hindemith.py:15).  Keys read here:
-#   hs_sweeps_per_pass  -- temporal-blocking depth T of the fused sweep (0 = default)
-#   hs_rows_per_segment -- rows per warp work item (0 = default)
+#   hs_sweeps_per_pass  -- temporal-blocking depth T of the fused sweep (0 or absent:
+#                          autotuned per shape and form, see hs_autotune)
+#   hs_rows_per_segment -- rows per warp work item (0 = the tuned or default value)
 #   hs_fast_math        -- True: FMA form (within 1e-4); False: bit-identical order
+#   hs_autotune         -- False: without hs_sweeps_per_pass, take the library's default
+#                          configuration instead of timing candidates on the first call
 # The reference's OpenCL launch-geometry keys (nd20, nt20, ne20, ...) are accepted and
 # ignored: launch geometry here is chosen per device.
 defines: Dict[str, Any] = {}

@@ -101,10 +101,13 @@ class Warp(torch.autograd.Function):
         H, W = src.shape
         g = _plane(g.to(torch.float32))
         buf = torch.empty((3, H, src.stride(0)), dtype=torch.float32, device=src.device)[:, :, :W]
-        buf[0].zero_()
-        L.check(L.lib().hs_warp_adjoint(D.ptr(src), D.ptr(u), D.ptr(v), D.ptr(g), H, W,
-                                        src.stride(0), D.ptr(buf[0]), D.ptr(buf[1]),
-                                        D.ptr(buf[2]), D.stream_handle()), "hs_warp_adjoint")
+        lib = L.lib()
+        ws = torch.empty(int(lib.hs_warp_adjoint_workspace_bytes(H, W, src.stride(0))),
+                         dtype=torch.uint8, device=src.device)
+        L.check(lib.hs_warp_adjoint(D.ptr(src), D.ptr(u), D.ptr(v), D.ptr(g), H, W,
+                                    src.stride(0), D.ptr(buf[0]), D.ptr(buf[1]),
+                                    D.ptr(buf[2]), D.ptr(ws), ws.numel(), D.stream_handle()),
+                "hs_warp_adjoint")
         return buf[0], buf[1], buf[2]
 
 

@@ -54,7 +54,10 @@ typedef enum hs_binop { HS_OP_ADD = 0, HS_OP_SUB = 1, HS_OP_MUL = 2, HS_OP_DIV =
 
 /* Tuning of the sweep kernels.  Zero-initialise for the defaults. */
 typedef struct hs_config {
-    int sweeps_per_pass;  /* temporal-blocking depth T (1..8) = sweeps per HBM pass; 0 = default */
+    int sweeps_per_pass;  /* temporal-blocking depth T (1..8) = sweeps per HBM pass; 0 = default:
+                           * for hs_forward / hs_sweeps / hs_forward_noalloc a measured table by
+                           * image size and form (within 6 % of the autotuned best on B200 from
+                           * 240x320 to 4096^2), 4 for the other calls */
     int rows_per_segment; /* rows each warp streams per work item; 0 = default */
     int fast_math;        /* 0 (default): the reference program's operation order, one
                              rounding per operation -- bit-identical to the reference's
@@ -170,9 +173,12 @@ HS_API size_t hs_checkpoint_bytes(int H, int W, int ld, int iters, int ckpt_ever
 HS_API size_t hs_forward_train_workspace_bytes(int H, int W, int ld);
 
 /* hs_forward that also keeps what the backward needs: `derivs` receives Ix, Iy, It and
- * `ckpt` the state (u, v) before sweeps 0, c, 2c, ... (c = ckpt_every).  `alpha` is a
- * DEVICE pointer to one float (a learnable alpha never needs a host round trip).
- * Results equal hs_forward's.  No counterpart in the reference, which has no gradients. */
+ * `ckpt` the state (u, v) before sweeps 0, c, 2c, ... (c = ckpt_every) and after the last
+ * sweep (hs_checkpoint_bytes: ceil(iters / c) + 1 plane pairs).  `alpha` is a DEVICE
+ * pointer to one float (a learnable alpha never needs a host round trip).  It runs the
+ * batched training passes with one pair (hs_forward_train_batched); the workspace
+ * (hs_forward_train_workspace_bytes) holds the passes' ping-pong planes.  Results equal
+ * hs_forward's.  No counterpart in the reference, which has no gradients. */
 HS_API hs_status hs_forward_train(const float *I0, const float *I1, int H, int W, int ld,
                                   const float *alpha, int iters, int ckpt_every, float *u,
                                   float *v, float *derivs, float *ckpt, void *workspace,
@@ -184,7 +190,8 @@ HS_API size_t hs_backward_workspace_bytes(int H, int W, int ld, int ckpt_every);
  * dL/dI0, dL/dI1 (planes) and dL/dalpha (one device float).  Each checkpoint interval's
  * states are recomputed from its checkpoint, then its sweeps are reversed with the
  * adjoint kernel (transposed clamp-to-edge average, adjoint of the pointwise update);
- * the derivative stencils are transposed last.  Deterministic. */
+ * the derivative stencils are transposed last.  The same passes as hs_backward_batched
+ * with one pair; needs alpha != 0.  Deterministic. */
 HS_API hs_status hs_backward(const float *derivs, int H, int W, int ld, const float *alpha,
                              int iters, int ckpt_every, const float *ckpt, const float *dLdu,
                              const float *dLdv, float *dI0, float *dI1, float *dalpha,
@@ -245,13 +252,19 @@ HS_API hs_status hs_upsample2_adjoint(const float *dfine, int H, int W, int ld, 
 /* dst = src backward-warped by the offsets (u, v) with WarpImg2D's semantics
  * (Operations/OpticalFlow/WarpImg2D.cpp:33-75): bilinear when the 2x2 footprint at
  * (x + u, y + v) lies inside the image, else the source pixel; bit-identical to the
- * template's float/double arithmetic.  The adjoint adds dL/dsrc into dsrc (atomic scatter)
- * and overwrites du, dv with dL/du, dL/dv (piecewise derivative). */
+ * template's float/double arithmetic.  The adjoint overwrites dsrc with dL/dsrc and du, dv
+ * with dL/du, dL/dv (piecewise derivative).  dL/dsrc is a scatter along the flow, summed
+ * as 64-bit fixed-point integers with one power-of-two scale per call (chosen from
+ * max |ddst| and max(|u|, |v|) so that no sum can overflow), hence deterministic: the same
+ * inputs give the same bits on every run.  Non-finite ddst or offsets give NaN in dsrc.
+ * The workspace (hs_warp_adjoint_workspace_bytes, 256-byte aligned) holds the sums. */
 HS_API hs_status hs_warp(const float *src, const float *u, const float *v, int H, int W, int ld,
                          float *dst, void *stream);
+HS_API size_t hs_warp_adjoint_workspace_bytes(int H, int W, int ld);
 HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *v,
                                  const float *ddst, int H, int W, int ld, float *dsrc, float *du,
-                                 float *dv, void *stream);
+                                 float *dv, void *workspace, size_t workspace_bytes,
+                                 void *stream);
 
 /* ---- Horn-Schunck as a linear system (CG family) ------------------------------ */
 

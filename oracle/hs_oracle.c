@@ -61,6 +61,15 @@ HSO_API int hso_num_threads(void) {
 #endif
 }
 
+/* Threads of the following parallel loops (the timed CPU legs run at 1 and at all cores). */
+HSO_API void hso_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
 /* ---------------------------------------------------------------- stencils */
 
 /* Stencil2DMVM.cpp:34-59, FP32, tap order. */

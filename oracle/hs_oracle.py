@@ -167,6 +167,7 @@ def lib():
         i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
         c_int, c_float, c_double = ctypes.c_int, ctypes.c_float, ctypes.c_double
         L.hso_num_threads.restype = c_int
+        L.hso_set_num_threads.argtypes = [c_int]
         L.hso_stencil2d_f32.argtypes = [f32p, i32p, i32p, c_int, f32p, f32p, c_int, c_int]
         L.hso_stencil2d_f64.argtypes = [f64p, i32p, i32p, c_int, f64p, f64p, c_int, c_int]
         L.hso_stencil2d_transpose_f64.argtypes = [f64p, i32p, i32p, c_int, f64p, f64p, c_int, c_int]
@@ -203,6 +204,11 @@ def _c64(a):
 
 def c_num_threads():
     return lib().hso_num_threads()
+
+
+def c_set_num_threads(n):
+    """OpenMP threads of the C restatement's loops from now on (n >= 1)."""
+    lib().hso_set_num_threads(int(n))
 
 
 def c_stencil2d(w, offx, offy, x, dtype=np.float32):
@@ -520,3 +526,25 @@ def warp_adjoint_f64(src, ox, oy, g):
     dox = go * ((1 - yf) * (s10 - s00) + yf * (s11 - s01))
     doy = go * ((1 - xf) * (s01 - s00) + xf * (s11 - s10))
     return dsrc, dox, doy
+
+
+def coarse_to_fine_f64(I0, I1, alpha, levels, iters):
+    """FP64 coarse-to-fine Horn-Schunck composed of the pieces above (the composition of
+    hindemith_b200.pyramid.coarse_to_fine): binomial pyramids, then from the coarsest
+    level up: upsample the flow (x2), warp I1 by it, run `iters` sweeps from zero on the
+    warped pair and add the increment.  HS sweeps are the C restatement in double."""
+    p0 = [np.asarray(I0, np.float64)]
+    p1 = [np.asarray(I1, np.float64)]
+    for _ in range(levels - 1):
+        p0.append(blur_down(p0[-1]))
+        p1.append(blur_down(p1[-1]))
+    u = v = None
+    for lev in range(levels - 1, -1, -1):
+        if u is None:
+            u, v = c_hs_forward(p0[lev], p1[lev], alpha, iters, np.float64)
+        else:
+            H, W = p0[lev].shape
+            uu, vv = upsample2(u, H, W), upsample2(v, H, W)
+            du, dv = c_hs_forward(p0[lev], warp_f64(p1[lev], uu, vv), alpha, iters, np.float64)
+            u, v = uu + du, vv + dv
+    return u, v

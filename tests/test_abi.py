@@ -148,7 +148,12 @@ def test_pyramid_argument_checks():
     assert lib.hs_upsample2_adjoint(P, 8, 8, 8, fake_ptr(4), 4, 2.0, None) == L.HS_ERR_ALIGNMENT
     assert lib.hs_warp(P, P, P, 8, 8, 8, P, None) == L.HS_ERR_INVALID_ARG
     assert lib.hs_warp(P, P, None, 8, 8, 8, Q, None) == L.HS_ERR_INVALID_ARG
-    assert lib.hs_warp_adjoint(P, P, P, P, 8, 7, 7, Q, Q, Q, None) == L.HS_ERR_ALIGNMENT
+    need = lib.hs_warp_adjoint_workspace_bytes(8, 8, 8)
+    assert need == 256 + 512
+    assert lib.hs_warp_adjoint(P, P, P, P, 8, 7, 7, Q, Q, Q, Q, need, None) == L.HS_ERR_ALIGNMENT
+    assert lib.hs_warp_adjoint(P, P, P, P, 8, 8, 8, Q, Q, Q, Q, need - 1, None) == L.HS_ERR_WORKSPACE
+    assert lib.hs_warp_adjoint(P, P, P, P, 8, 8, 8, Q, Q, Q, None, need, None) == L.HS_ERR_WORKSPACE
+    assert lib.hs_warp_adjoint(P, P, P, P, 8, 8, 8, Q, Q, Q, fake_ptr(16), need, None) == L.HS_ERR_ALIGNMENT
 
 
 def test_epe_argument_checks_before_launch():

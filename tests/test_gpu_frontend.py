@@ -106,3 +106,33 @@ def test_stencil_mul_outside_hm(cuda):
     y = A * x
     assert isinstance(y, np.ndarray)
     assert_bitexact(y, d["out4"], "A*x")
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_hm_without_defines_runs_the_tuned_sweep(cuda, fast):
+    """With no depth in `defines`, the fused loop runs the configuration the autotuner picks
+    for the shape and form; the exact form stays bit-identical to the golden fixture, the
+    fast form within 1e-4 of it."""
+    from hindemith_b200 import autotune
+    from hindemith_b200 import defines
+
+    d = golden("hs_70x130.npz")
+    old = dict(defines)
+    try:
+        defines.clear()
+        if fast:
+            defines["hs_fast_math"] = True
+        f = hm(hs_programs.hs_jacobi)
+        u, v = f(**kwargs_for(d, alpha2=np.float32(d["alpha2"]), sweeps=np.int64(d["sweeps"])))
+        ex = next(iter(f._cache.values()))
+    finally:
+        defines.clear()
+        defines.update(old)
+    H, W = d["I0"].shape
+    T, seg, layout = autotune.best_sweep_config(H, W, (W + 3) // 4 * 4, fast_math=fast)
+    assert ex.last_sweep_config == (T, seg, layout, fast)
+    if fast:
+        assert np.abs(u - d["u"]).max() < 1e-4 and np.abs(v - d["v"]).max() < 1e-4
+    else:
+        assert_bitexact(u, d["u"], "u")
+        assert_bitexact(v, d["v"], "v")

@@ -268,3 +268,18 @@ def test_lk_oracle_matches_float64_restatement():
         scale = max(np.abs(rdu).max(), np.abs(rdv).max(), 1e-6)
         assert np.abs(du - rdu).max() < 1e-4 * scale
         assert np.abs(dv - rdv).max() < 1e-4 * scale
+
+
+def test_coarse_to_fine_f64_matches_torch_float64():
+    """The FP64 coarse-to-fine composition the benchmark checks config-4 flows against
+    equals the float64 PyTorch composition of the same pieces."""
+    import torch
+
+    from hindemith_b200 import synthetic
+    from hs_torch_ref import coarse_to_fine_torch
+
+    I0, I1, _, _ = synthetic.make_pair(48, 64, seed=21, amplitude=4.0)
+    u, v = O.coarse_to_fine_f64(I0, I1, 1.0, 3, 15)
+    ur, vr = coarse_to_fine_torch(torch.from_numpy(I0.astype(np.float64)),
+                                  torch.from_numpy(I1.astype(np.float64)), 1.0, 3, 15)
+    assert np.abs(u - ur.numpy()).max() < 1e-9 and np.abs(v - vr.numpy()).max() < 1e-9
