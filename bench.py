@@ -3,8 +3,9 @@
 
 Workload (default): one 1920x1080 FP32 pair (blur 3 px, flow up to 2 px, seed 1000 +
 rank), alpha 1, 500 Jacobi sweeps, temporally blocked.  One step = one
-hs_forward call (derivatives + 500 sweeps) with the inputs already in HBM.  Between
-steps a 256 MiB buffer is written to flush L2.
+hs_forward call (derivatives + 500 sweeps) with the inputs already in HBM, captured once
+as a CUDA graph and replayed (the eager call is timed beside it).  Between steps a
+256 MiB buffer is written to flush L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -496,8 +497,36 @@ def measure_train(args, rank, flush, checks=None):
 
     stream = torch.cuda.current_stream()
     k = max(1, args.steps // 4)
-    t_f = timed_events(fwd, k, 3, flush, stream, "timed_train_fwd")
-    t_fb = timed_events(fwd_bwd, k, 3, flush, stream, "timed_train_fwd_bwd")
+    t_f_eager = timed_events(fwd, k, 3, flush, stream, "timed_train_fwd_eager")
+    t_fb_eager = timed_events(fwd_bwd, k, 3, flush, stream, "timed_train_fwd_bwd_eager")
+
+    # Both as CUDA graphs: a launch of this workload's passes takes about 50 us of device
+    # time, close to what the host needs to enqueue one, so the eager timings carry host
+    # time.  The graphs hold the same launches.
+    def fwd_bwd_fn():
+        # fresh leaves per call: an autograd leaf remembers the stream it was first used on
+        a = alpha.detach().requires_grad_(True)
+        xs = [(d[0].detach().requires_grad_(True), d[1].detach().requires_grad_(True)) for d in data]
+        outs = horn_schunck_batch(xs, a, 200, 10, cfg)
+        loss = mean_epe_batch(outs, [(d[2], d[3]) for d in data])
+        return (loss, *torch.autograd.grad(loss, [a] + [t for p in xs for t in p]))
+
+    graphs = []
+    for fn in (fwd, fwd_bwd_fn):
+        side = torch.cuda.Stream()
+        side.wait_stream(stream)
+        with torch.cuda.stream(side):
+            fn()
+        stream.wait_stream(side)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            keep = fn()
+        graphs.append((g, keep))
+    torch.cuda.synchronize()
+    t_f = timed_events(graphs[0][0].replay, k, 3, flush, stream, "timed_train_fwd")
+    t_fb = timed_events(graphs[1][0].replay, k, 3, flush, stream, "timed_train_fwd_bwd")
+    del graphs
     px_it = sum(sp.H * sp.W * sp.iters for sp in specs)
 
     # the single-pair form (horn_schunck: hs_forward_train + hs_backward) on pair 0
@@ -536,8 +565,12 @@ def measure_train(args, rank, flush, checks=None):
                                   "sweeps, checkpoints every 10, mean EPE, the timed config"}
     return {"workload": "hs_train_16x512x512_200sweeps_ckpt10", "pix_iters": px_it,
             "sweeps_per_pass": T, "api": "horn_schunck_batch (hs_forward_train_batched + hs_backward_batched) + mean_epe_batch",
+            "timed": "forward, and forward + loss + backward, each captured once as a CUDA graph "
+                     "and replayed",
             "fwd_ms": t_f / k * 1e3, "fwd_bwd_ms": t_fb / k * 1e3,
             "fwd_bwd_over_fwd": t_fb / t_f,
+            "eager": {"fwd_ms": t_f_eager / k * 1e3, "fwd_bwd_ms": t_fb_eager / k * 1e3,
+                      "fwd_bwd_over_fwd": t_fb_eager / t_f_eager},
             "fwd_value": px_it * k / t_f / 1e6,
             "value": px_it * k / t_fb / 1e6, "unit": UNIT + " (forward+backward)",
             "single_pair": single}
@@ -790,7 +823,9 @@ def measure_cg(args, rank, flush, peak):
     t_mp = timed_events(powers, k, 3, flush, stream, "timed_matrix_powers")
     t_pc = timed_events(precond, k, 3, flush, stream, "timed_preconditioner")
     passes = (steps - 1 + depth - 1) // depth
-    mp_bytes = H * W * (16 * passes + 8 * (steps - 1) + 16)  # + the copy of V[0]
+    # each pass reads one power (u, v) and Ix, Iy: 16 B/px; every power V[0..steps-1] is
+    # written once: 8 B/px each (V[0] by the first pass, from the r it reads)
+    mp_bytes = H * W * (16 * passes + 8 * steps)
     pc_bytes = H * W * 28
     mp_gbs = mp_bytes * k / t_mp / 1e9
     pc_gbs = pc_bytes * k / t_pc / 1e9
@@ -959,8 +994,23 @@ def main():
         torch.cuda.synchronize()
         return sum(a.elapsed_time(b) for a, b in evs) / 1e3  # seconds
 
+    # The step (derivatives, zeroing, all passes: one hs_forward call) as one CUDA graph, so
+    # that host launch jitter stays out of the device timing; the eager call is timed too.
+    side = torch.cuda.Stream()
+    side.wait_stream(stream)
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            step()
+    stream.wait_stream(side)
+    torch.cuda.synchronize()
+    step_graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(step_graph):
+        step()
+    torch.cuda.synchronize()
+
     with ClockSampler(torch.cuda.current_device()) as clk:
-        t_step = timed(step, args.steps, warmup, "timed_step")
+        t_step = timed(step_graph.replay, args.steps, warmup, "timed_step")
+        t_step_eager = timed(step, args.steps, warmup, "timed_step_eager")
         # sweep passes alone (the dominant kernel), same configuration, for the roofline
         Ixyt = D.hs_derivs(I0, I1)
         us, vs = D.empty_planes(2, H, W)
@@ -1015,7 +1065,7 @@ def main():
                             "exact": (eu.cpu().numpy(), ev.cpu().numpy()),
                             "exact_cfg": "hs_config zeroed (library default)"}
 
-    t_step, t_sweeps, t_e2e = max_over_ranks([t_step, t_sweeps, t_e2e])
+    t_step, t_step_eager, t_sweeps, t_e2e = max_over_ranks([t_step, t_step_eager, t_sweeps, t_e2e])
     if t_exact is not None:
         t_exact = max_over_ranks([t_exact])[0]
 
@@ -1068,6 +1118,10 @@ def main():
                 "pipeline": "pinned host -> device -> pinned host every step; copy-in and "
                             "copy-out streams overlap step k+1's and k-1's copies with step k's "
                             "sweeps"},
+        "step": {"timed": "one hs_forward call per step, captured once as a CUDA graph and "
+                          "replayed (the eager call beside it)",
+                 "eager_ms_per_step": t_step_eager / args.steps * 1e3,
+                 "eager_value": job_rate(H * W * iters * args.steps, world, t_step_eager) / 1e6},
         "exact_form": (None if t_exact is None else
                        {"value": H * W * iters * max(1, args.steps // 2) / t_exact / 1e6,
                         "unit": UNIT, "sweeps_per_pass": Te, "rows_per_segment": sege,

@@ -121,52 +121,49 @@ __device__ __forceinline__ void st_release(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Poll `flag` until it reaches `need`, with exponential nanosleep back-off; gives up (false)
-// after `max_polls` polls in all (`polls` carries the count across calls) or when
-// *abort_flag is raised.
-__device__ bool wait_flag_ge(const unsigned *flag, unsigned need, const unsigned *abort_flag,
-                             unsigned long long max_polls, unsigned long long &polls, unsigned &ns) {
-    while (ld_acquire(flag) < need) {
-        if (++polls > max_polls) return false;
-        if ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag) return false;
+// Bounded warp-wide wait: each lane watches `flag` (nullptr: nothing to wait for) until it
+// reaches `need`; one round of acquire loads checks every lane's flag, with an exponential
+// nanosleep back-off (32 .. 256 ns) between rounds.  Gives up (false on every lane) after
+// `max_polls` rounds or when *abort_flag is raised.
+__device__ bool warp_wait_ge(const unsigned *flag, unsigned need, const unsigned *abort_flag,
+                             unsigned long long max_polls, int lane) {
+    unsigned long long polls = 0;
+    unsigned ns = 32;
+    for (;;) {
+        const bool done = flag == nullptr || ld_acquire(flag) >= need;
+        if (__all_sync(kFull, done)) return true;
+        ++polls;
+        int stop = 0;
+        if (lane == 0)
+            stop = polls > max_polls || ((polls & 63) == 0 && *(volatile const unsigned *)abort_flag);
+        if (__shfl_sync(kFull, stop, 0)) return false;
         __nanosleep(ns);
         ns = min(ns * 2, 256u);
     }
-    return true;
 }
 
-// Lane 0: wait until tiles (seg+-1, strip+-1) of pair P have completed `need` passes.
-// Returns false if the wait gave up or another warp aborted.
+// The warp waits until tiles (seg+-1, strip+-1) of pair P have completed `need` passes:
+// lane i < 9 watches neighbour i.  Returns false if the wait gave up or another warp aborted.
 __device__ bool wait_neighbours(const BatchPair &P, int seg, int strip, unsigned need,
-                                const unsigned *abort_flag) {
+                                const unsigned *abort_flag, int lane) {
     const int nseg = (P.H + P.seg_rows - 1) / P.seg_rows;
-    unsigned long long polls = 0;
-    unsigned ns = 32;
-    for (int dg = -1; dg <= 1; ++dg) {
-        const int g = seg + dg;
-        if (g < 0 || g >= nseg) continue;
-        for (int ds = -1; ds <= 1; ++ds) {
-            const int s = strip + ds;
-            if (s < 0 || s >= P.nstrips) continue;
-            const unsigned *flag = P.progress + (size_t)g * P.nstrips + s;
-            if (!wait_flag_ge(flag, need, abort_flag, kWaitPolls, polls, ns)) return false;
-        }
-    }
-    return true;
+    const int g = seg + lane / 3 - 1, s = strip + lane % 3 - 1;
+    const bool mine = lane < 9 && g >= 0 && g < nseg && s >= 0 && s < P.nstrips;
+    return warp_wait_ge(mine ? P.progress + (size_t)g * P.nstrips + s : nullptr, need, abort_flag,
+                        kWaitPolls, lane);
 }
 
-// Self-test of the failure path: one thread waits, with the batched kernel's bounded wait,
-// on a flag that no code ever sets; the wait gives up and reports HS_ERR_TIMEOUT through
+// Self-test of the failure path: one warp runs the batched kernel's bounded wait with lane 0
+// watching a flag that no code ever sets; the wait gives up and reports HS_ERR_TIMEOUT through
 // the status word, and the kernel returns (the context stays usable).
 __device__ unsigned g_never_set_flag = 0;
 __device__ unsigned g_selftest_abort = 0;
 
 __global__ void wait_selftest_kernel(int *status, unsigned long long max_polls) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    unsigned long long polls = 0;
-    unsigned ns = 32;
-    if (!wait_flag_ge(&g_never_set_flag, 1u, &g_selftest_abort, max_polls, polls, ns))
-        atomicCAS(status, 0, (int)HS_ERR_TIMEOUT);
+    const int lane = threadIdx.x & 31;
+    if (blockIdx.x != 0 || threadIdx.x >= 32) return;  // one whole warp
+    if (!warp_wait_ge(lane == 0 ? &g_never_set_flag : nullptr, 1u, &g_selftest_abort, max_polls, lane))
+        if (lane == 0) atomicCAS(status, 0, (int)HS_ERR_TIMEOUT);
 }
 
 // (pass, pair, local tile) of work item `g`: the last unit whose first item is <= g.
@@ -213,16 +210,16 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (batch_min_blocks<T, WIDE
         const int strip = local % P.nstrips;
         const int seg = local / P.nstrips;
         int ok = 1;
-        if (lane == 0) {
-            ok = (*(volatile const unsigned *)bp.abort_flag == 0);
-            if (ok && pass > 0) ok = wait_neighbours(P, seg, strip, (unsigned)pass, bp.abort_flag);
-            if (!ok) {
+        if (lane == 0) ok = (*(volatile const unsigned *)bp.abort_flag == 0);
+        ok = __shfl_sync(kFull, ok, 0);
+        if (ok && pass > 0) ok = wait_neighbours(P, seg, strip, (unsigned)pass, bp.abort_flag, lane);
+        if (!ok) {
+            if (lane == 0) {
                 atomicCAS(bp.status, 0, (int)HS_ERR_TIMEOUT);
                 atomicExch(bp.abort_flag, 1u);
             }
+            break;
         }
-        ok = __shfl_sync(kFull, ok, 0);
-        if (!ok) break;
         __syncwarp();
 
         SweepParams sp;

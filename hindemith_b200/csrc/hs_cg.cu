@@ -6,159 +6,192 @@
 //   M (u, v) = (Ix g, Iy g) + lam * (deg*mid - sum of the present 4-neighbours), g = Ix u + Iy v
 // evaluated in the operation order of HSMatrixPowers.cpp:72-106 (one rounding each), so the
 // result is bit-identical to the reference's FP32 semantics.  Every power is an output, so
-// a pass cannot skip writes; what temporal blocking saves is the reads: a CTA loads a
-// (64 + 8) x (32 + 2T) tile of u, v, Ix, Iy once into shared memory, advances it T powers
-// there (the valid region shrinks by one cell per power) and writes each power's 64 x 32 core.
-// Per power that is 8 B/px written plus (16 B/px x halo overhead) / T read, against
-// 24 B/px for one launch per power.
+// a pass cannot skip writes; what temporal blocking saves is the reads.  A pass of D powers
+// streams the strip down the image like the Jacobi sweep (hs_stream4.cuh): a warp owns a
+// 128-column strip (4 columns per lane) of a segment of rows, D stages form a register
+// pipeline (stage s turns row n of power s0+s into row n-1 of power s0+s+1 and writes it),
+// each stage keeps its two previous input rows in registers, and only the two lane-edge
+// columns cross lanes (shuffles).  Per power that is 8 B/px written plus 16 B/px / D read
+// (plus the strips' 4-column halos).
 #include <algorithm>
 
-#include "hs_common.cuh"
+#include "hs_stream.cuh"
 
 namespace hs {
 
-constexpr int kMpTX = 64;       // output tile width
-constexpr int kMpTY = 32;       // output tile height
-constexpr int kMpHX = 4;        // halo columns each side (>= depth; 16-byte aligned loads)
-constexpr int kMpMaxDepth = 4;  // powers per pass
-constexpr int kMpThreads = 256;
+constexpr int kMpMaxDepth = 4;                     // powers per pass
+constexpr int kMpCols = 128;                       // strip width (4 columns per lane)
+constexpr int kMpHalo = 4;                         // >= depth; keeps chunks 16-byte aligned
+constexpr int kMpStrip = kMpCols - 2 * kMpHalo;    // output columns per strip
+constexpr int kMpPrefetch = 2;                     // rows in flight per warp
+constexpr int kMpPlanes = 4;                       // u, v, Ix, Iy
+constexpr int kMpWarps = 4;                        // warps per CTA
 
 template <int D>
 struct MpGeo {
-    static constexpr int EX = kMpTX + 2 * kMpHX;  // tile width with halo
-    static constexpr int EY = kMpTY + 2 * D;      // tile height with halo
-    static constexpr int N = EX * EY;
-    static constexpr int smem_bytes = 6 * N * (int)sizeof(float);  // Ix, Iy, u0, v0, u1, v1
+    // ring of rows: stage s at step k reads Ix, Iy of row k-s-1, so rows k-D .. k+prefetch
+    static constexpr int slots = D + 1 + kMpPrefetch;
+    static constexpr int warp_floats = slots * kMpPlanes * kMpCols;
+    static constexpr int smem_bytes = kMpWarps * warp_floats * (int)sizeof(float);
 };
 
-// One power at one cell from the previous power in shared memory (row stride E); the
-// neighbour tests use image coordinates, as the template's element_id tests do.
-__device__ __forceinline__ void mp_cell(const float *u, const float *v, const float *Ix,
-                                        const float *Iy, int c, int E, int x, int y, int H, int W,
-                                        float lam, float &ur, float &vr) {
-    const float um = u[c], vm = v[c], ix = Ix[c], iy = Iy[c];
-    const float g = __fadd_rn(__fmul_rn(ix, um), __fmul_rn(iy, vm));
-    ur = __fmul_rn(ix, g);
-    vr = __fmul_rn(iy, g);
-    const float nl = -lam;
-    const float lu = __fmul_rn(lam, um), lv = __fmul_rn(lam, vm);
-    if (x > 0) {
-        ur = __fadd_rn(__fadd_rn(ur, __fmul_rn(nl, u[c - 1])), lu);
-        vr = __fadd_rn(__fadd_rn(vr, __fmul_rn(nl, v[c - 1])), lv);
-    }
-    if (x < W - 1) {
-        ur = __fadd_rn(__fadd_rn(ur, __fmul_rn(nl, u[c + 1])), lu);
-        vr = __fadd_rn(__fadd_rn(vr, __fmul_rn(nl, v[c + 1])), lv);
-    }
-    if (y > 0) {
-        ur = __fadd_rn(__fadd_rn(ur, __fmul_rn(nl, u[c - E])), lu);
-        vr = __fadd_rn(__fadd_rn(vr, __fmul_rn(nl, v[c - E])), lv);
-    }
-    if (y < H - 1) {
-        ur = __fadd_rn(__fadd_rn(ur, __fmul_rn(nl, u[c + E])), lu);
-        vr = __fadd_rn(__fadd_rn(vr, __fmul_rn(nl, v[c + E])), lv);
-    }
+struct MpParams {
+    const float *Ix, *Iy, *u_in, *v_in;
+    float *V0, *V1;     // power s0 of the pass (V[s0]); power s0+j at + j * pstride
+    size_t pstride;
+    int H, W, ld, seg_rows, nstrips, nitems;
+    float lam;
+    int copy0;          // also write the input rows as power s0 (V[0] = r on the first pass)
+};
+
+// One cell of one power (HSMatrixPowers.cpp:72-106 order): m = (u, v) at the cell,
+// l / r / up / dn its neighbours, present per the flags.  The u and v chains run as one
+// packed pair: the products are scalar (mul2r: rounded on their own, never fused) and the
+// adds packed (add.rn.f32x2: each half one IEEE add), so every operation rounds exactly as
+// the template's scalar code.
+__device__ __forceinline__ float2 mp_cell(float ix, float iy, float2 m, float2 l, float2 r,
+                                          float2 up, float2 dn, bool hl, bool hr, bool hu, bool hd,
+                                          float lam) {
+    const float g = __fadd_rn(__fmul_rn(ix, m.x), __fmul_rn(iy, m.y));
+    float2 o = mul2r(f2(ix, iy), f2(g, g));
+    const float2 nl = f2(-lam, -lam);
+    const float2 lm = mul2r(f2(lam, lam), m);
+    if (hl) o = add2(add2(o, mul2r(nl, l)), lm);
+    if (hr) o = add2(add2(o, mul2r(nl, r)), lm);
+    if (hu) o = add2(add2(o, mul2r(nl, up)), lm);
+    if (hd) o = add2(add2(o, mul2r(nl, dn)), lm);
+    return o;
 }
 
-// One power over the tile region [x0, x0+SX) x [y0, y0+SY) (tile coordinates), flattened
-// over the CTA's threads.  INTERIOR: the whole tile lies at least one cell inside the image,
-// so every computed cell has its four neighbours and no test is needed.
-template <int EX, int SX, int SY, bool INTERIOR>
-__device__ __forceinline__ void mp_region(const float *u, const float *v, const float *sIx,
-                                          const float *sIy, float *uo, float *vo, int x0, int y0,
-                                          int tx0, int ty0, int H, int W, float lam) {
-    for (int k = threadIdx.x; k < SX * SY; k += kMpThreads) {
-        const int cy = y0 + k / SX, cx = x0 + k % SX;
-        const int c = cy * EX + cx;
-        float ur, vr;
-        if constexpr (INTERIOR) {
-            mp_cell(u, v, sIx, sIy, c, EX, 1, 1, 3, 3, lam, ur, vr);  // all neighbours present
-        } else {
-            const int x = tx0 + cx, y = ty0 + cy;
-            if (x < 0 || x >= W || y < 0 || y >= H) continue;
-            mp_cell(u, v, sIx, sIy, c, EX, x, y, H, W, lam, ur, vr);
-        }
-        uo[c] = ur;
-        vo[c] = vr;
-    }
+// A stage's window: its two previous input rows (4 columns of u and v), the middle row's
+// neighbours across the lane edges.
+struct MpWin {
+    float4 uu, vu;        // row n-2
+    float4 um, vm;        // row n-1
+    float ml_u, ml_v;     // row n-1, column xa-1
+    float mr_u, mr_v;     // row n-1, column xa+4
+};
+
+__device__ __forceinline__ float4 f4get(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float f4at(const float4 &a, int j) {
+    return j == 0 ? a.x : (j == 1 ? a.y : (j == 2 ? a.z : a.w));
 }
 
-// Power T of a pass of D (T = 1 .. D, unrolled at compile time): compute it over the
-// region still needed by the later powers, then store its core.
-template <int D, int T>
-__device__ __forceinline__ void mp_power(float *sIx, float *sIy, float *su0, float *sv0, float *su1,
-                                         float *sv1, bool interior, int tx0, int ty0, int H, int W,
-                                         int ld, float lam, float *V0, float *V1, size_t pstride) {
-    constexpr int EX = MpGeo<D>::EX;
-    constexpr int M = D - T;  // power T is needed within M cells of the core
-    constexpr int SX = kMpTX + 2 * M, SY = kMpTY + 2 * M;
-    constexpr bool odd = T & 1;
-    const float *u = odd ? su0 : su1, *v = odd ? sv0 : sv1;
-    float *uo = odd ? su1 : su0, *vo = odd ? sv1 : sv0;
-    if (interior)
-        mp_region<EX, SX, SY, true>(u, v, sIx, sIy, uo, vo, kMpHX - M, D - M, tx0, ty0, H, W, lam);
-    else
-        mp_region<EX, SX, SY, false>(u, v, sIx, sIy, uo, vo, kMpHX - M, D - M, tx0, ty0, H, W, lam);
-    __syncthreads();
-    // store the core (the next power reads uo as well and writes the other buffer)
-    float *out0 = V0 + (size_t)T * pstride, *out1 = V1 + (size_t)T * pstride;
-    for (int k = threadIdx.x; k < (kMpTX / 4) * kMpTY; k += kMpThreads) {
-        const int gx = k % (kMpTX / 4), cy = D + k / (kMpTX / 4);
-        const int x = tx0 + kMpHX + 4 * gx, y = ty0 + cy;
-        if (x >= W || y >= H) continue;
-        const int c = cy * EX + kMpHX + 4 * gx;
-        const size_t o = (size_t)y * ld + x;
-        if (x + 4 <= W) {
-            *reinterpret_cast<float4 *>(out0 + o) = *reinterpret_cast<const float4 *>(uo + c);
-            *reinterpret_cast<float4 *>(out1 + o) = *reinterpret_cast<const float4 *>(vo + c);
-        } else {
-            for (int j = 0; j < W - x; ++j) {
-                out0[o + j] = uo[c + j];
-                out1[o + j] = vo[c + j];
-            }
-        }
-    }
-    if constexpr (T < D)
-        mp_power<D, T + 1>(sIx, sIy, su0, sv0, su1, sv1, interior, tx0, ty0, H, W, ld, lam, V0, V1,
-                           pstride);
-}
+// three CTAs (12 warps) per SM: the depth-4 pass needs 167 registers and 57 KB of shared
+// memory per CTA
+constexpr int kMpBlocksPerSm = 3;
 
-// D powers: V[s0+1 .. s0+D] from V[s0].  Loads and stores move 16-byte groups (the tile's
-// first column is a multiple of 4, rows start 16-byte aligned); tile cells outside the image
-// load as 0 and are never read by an in-image cell (the neighbour tests skip them).
 template <int D>
-__global__ void __launch_bounds__(kMpThreads) mp_pass_kernel(float lam, const float *__restrict__ Ix,
-                                                             const float *__restrict__ Iy,
-                                                             const float *u_in, const float *v_in,
-                                                             float *V0, float *V1, size_t pstride,
-                                                             int H, int W, int ld) {
+__global__ void __launch_bounds__(kMpWarps * 32, kMpBlocksPerSm) mp_stream_kernel(const MpParams p) {
     using G = MpGeo<D>;
-    constexpr int EX = G::EX, EY = G::EY, GX = EX / 4;
     extern __shared__ float4 sm4[];
-    float *sm = reinterpret_cast<float *>(sm4);
-    float *sIx = sm, *sIy = sm + G::N;
-    float *su0 = sm + 2 * G::N, *sv0 = sm + 3 * G::N, *su1 = sm + 4 * G::N, *sv1 = sm + 5 * G::N;
-    const int tx0 = blockIdx.x * kMpTX - kMpHX, ty0 = blockIdx.y * kMpTY - D;
-    const bool interior = tx0 >= 1 && ty0 >= 1 && tx0 + EX <= W - 1 && ty0 + EY <= H - 1;
-    for (int c = threadIdx.x; c < GX * EY; c += kMpThreads) {
-        const int gx = c % GX, cy = c / GX;
-        const int x = tx0 + 4 * gx, y = ty0 + cy;
-        float4 a = make_float4(0.f, 0.f, 0.f, 0.f), b = a, p = a, q = a;
-        if (x >= 0 && x + 4 <= ld && y >= 0 && y < H) {
-            const size_t o = (size_t)y * ld + x;
-            a = __ldg(reinterpret_cast<const float4 *>(Ix + o));
-            b = __ldg(reinterpret_cast<const float4 *>(Iy + o));
-            p = *reinterpret_cast<const float4 *>(u_in + o);
-            q = *reinterpret_cast<const float4 *>(v_in + o);
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    float *ring = reinterpret_cast<float *>(sm4) + warp * G::warp_floats;
+    const int item = blockIdx.x * kMpWarps + warp;
+    if (item >= p.nitems) return;  // warp-uniform
+    const int strip = item % p.nstrips, seg = item / p.nstrips;
+    const int xa = strip * kMpStrip - kMpHalo + 4 * lane;  // first of the lane's 4 columns
+    const int lcol = (xa >= 0 && xa + 4 <= p.ld) ? xa : 0;  // any in-bounds chunk otherwise
+    const int vlo = strip * kMpStrip, vhi = min(vlo + kMpStrip, p.W);
+    unsigned st = 0u;  // bit j: column xa+j is stored by this strip
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (xa + j >= vlo && xa + j < vhi) st |= 1u << j;
+    const int y_start = seg * p.seg_rows, y_end = min(p.H, y_start + p.seg_rows);
+    const int k0 = max(0, y_start - D), k_end = y_end - 1 + D;
+    const int last_row = y_end - 1 + D;  // rows past it are never needed
+
+    auto issue = [&](int row) {
+        const int slot = ((row % G::slots) + G::slots) % G::slots;
+        const int r = min(max(row, 0), p.H - 1);
+        const size_t off = (size_t)r * p.ld + lcol;
+        float *b = ring + slot * (kMpPlanes * kMpCols) + 4 * lane;
+        cp_async16(b + 0 * kMpCols, p.u_in + off);
+        cp_async16(b + 1 * kMpCols, p.v_in + off);
+        cp_async16(b + 2 * kMpCols, p.Ix + off);
+        cp_async16(b + 3 * kMpCols, p.Iy + off);
+        cp_async_commit();
+    };
+    auto store = [&](float *U, float *V, int r, float4 a, float4 b) {
+        if (r < y_start || r >= y_end || st == 0u) return;
+        const size_t o = (size_t)r * p.ld + xa;
+        if (st == 15u) {
+            *reinterpret_cast<float4 *>(U + o) = a;
+            *reinterpret_cast<float4 *>(V + o) = b;
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (st & (1u << j)) {
+                    U[o + j] = f4at(a, j);
+                    V[o + j] = f4at(b, j);
+                }
         }
-        const int k = cy * EX + 4 * gx;
-        *reinterpret_cast<float4 *>(sIx + k) = a;
-        *reinterpret_cast<float4 *>(sIy + k) = b;
-        *reinterpret_cast<float4 *>(su0 + k) = p;
-        *reinterpret_cast<float4 *>(sv0 + k) = q;
+    };
+
+    MpWin w[D];
+#pragma unroll
+    for (int s = 0; s < D; ++s) w[s] = MpWin{};
+#pragma unroll
+    for (int i = 0; i < kMpPrefetch; ++i) issue(k0 + i);
+    for (int k = k0; k <= k_end; ++k) {
+        issue(min(k + kMpPrefetch, last_row));
+        cp_async_wait<kMpPrefetch>();
+        const float *row_k = ring + (k % G::slots) * (kMpPlanes * kMpCols) + 4 * lane;
+        float4 cu = f4get(row_k), cv = f4get(row_k + kMpCols);  // row k of power s0
+        if (p.copy0) store(p.V0, p.V1, k, cu, cv);
+#pragma unroll
+        for (int s = 0; s < D; ++s) {
+            MpWin &q = w[s];
+            const int n = k - s;     // arriving row of power s0+s
+            const int r = n - 1;     // the row this stage emits (power s0+s+1)
+            const float *row_r = ring + (((r % G::slots) + G::slots) % G::slots) * (kMpPlanes * kMpCols) + 4 * lane;
+            const float4 ix = f4get(row_r + 2 * kMpCols), iy = f4get(row_r + 3 * kMpCols);
+            const bool hu = r > 0, hd = r < p.H - 1;
+            float4 ou, ov;
+            float *o_u = &ou.x, *o_v = &ov.x;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int x = xa + j;
+                const float2 l = j == 0 ? f2(q.ml_u, q.ml_v) : f2(f4at(q.um, j - 1), f4at(q.vm, j - 1));
+                const float2 rr = j == 3 ? f2(q.mr_u, q.mr_v) : f2(f4at(q.um, j + 1), f4at(q.vm, j + 1));
+                const float2 o = mp_cell(f4at(ix, j), f4at(iy, j), f2(f4at(q.um, j), f4at(q.vm, j)), l, rr,
+                                         f2(f4at(q.uu, j), f4at(q.vu, j)), f2(f4at(cu, j), f4at(cv, j)),
+                                         x > 0, x < p.W - 1, hu, hd, p.lam);
+                o_u[j] = o.x;
+                o_v[j] = o.y;
+            }
+            // advance the window: row n becomes the middle row, with its lane-edge neighbours
+            q.uu = q.um;
+            q.vu = q.vm;
+            q.um = cu;
+            q.vm = cv;
+            q.ml_u = __shfl_up_sync(kFull, cu.w, 1);
+            q.ml_v = __shfl_up_sync(kFull, cv.w, 1);
+            q.mr_u = __shfl_down_sync(kFull, cu.x, 1);
+            q.mr_v = __shfl_down_sync(kFull, cv.x, 1);
+            store(p.V0 + (size_t)(s + 1) * p.pstride, p.V1 + (size_t)(s + 1) * p.pstride, r, ou, ov);
+            cu = ou;
+            cv = ov;
+        }
     }
-    __syncthreads();
-    mp_power<D, 1>(sIx, sIy, su0, sv0, su1, sv1, interior, tx0, ty0, H, W, ld, lam, V0, V1, pstride);
+    cp_async_wait<0>();
+}
+
+template <int D>
+static hs_status launch_mp(const MpParams &pp, cudaStream_t s) {
+    static bool attr[64] = {};
+    int dev = 0;
+    HS_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 64 && !attr[dev]) {
+        HS_CUDA_CHECK(cudaFuncSetAttribute(mp_stream_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           MpGeo<D>::smem_bytes));
+        attr[dev] = true;
+    }
+    const unsigned blocks = (unsigned)((pp.nitems + kMpWarps - 1) / kMpWarps);
+    mp_stream_kernel<D><<<blocks, kMpWarps * 32, MpGeo<D>::smem_bytes, s>>>(pp);
+    HS_LAUNCH_CHECK("mp_stream_kernel");
+    return HS_OK;
 }
 
 __device__ __forceinline__ void precond_px(float s2, float a, float d, float b, float e, float f,
@@ -216,25 +249,6 @@ __global__ void __launch_bounds__(256) precond_kernel(float s2, const float *__r
     }
 }
 
-template <int D>
-static hs_status launch_mp(float lam, const float *Ix, const float *Iy, const float *u,
-                           const float *v, float *V0, float *V1, size_t pstride, int H, int W,
-                           int ld, cudaStream_t s) {
-    static bool attr[64] = {};
-    int dev = 0;
-    HS_CUDA_CHECK(cudaGetDevice(&dev));
-    if (dev < 64 && !attr[dev]) {
-        HS_CUDA_CHECK(cudaFuncSetAttribute(mp_pass_kernel<D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           MpGeo<D>::smem_bytes));
-        attr[dev] = true;
-    }
-    const dim3 grid((unsigned)((W + kMpTX - 1) / kMpTX), (unsigned)((H + kMpTY - 1) / kMpTY));
-    mp_pass_kernel<D><<<grid, kMpThreads, MpGeo<D>::smem_bytes, s>>>(lam, Ix, Iy, u, v, V0, V1,
-                                                                      pstride, H, W, ld);
-    HS_LAUNCH_CHECK("mp_pass_kernel");
-    return HS_OK;
-}
-
 }  // namespace hs
 
 using namespace hs;
@@ -258,16 +272,41 @@ hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const fl
     if (depth > kMpMaxDepth) HS_FAIL(HS_ERR_INVALID_ARG, "sweeps_per_pass=%d outside 1..%d", depth, kMpMaxDepth);
     cudaStream_t s = (cudaStream_t)stream;
     const size_t row = (size_t)W * sizeof(float), pitch = (size_t)ld * sizeof(float);
-    if (V0 != r0) HS_CUDA_CHECK(cudaMemcpy2DAsync(V0, pitch, r0, pitch, row, H, cudaMemcpyDeviceToDevice, s));
-    if (V1 != r1) HS_CUDA_CHECK(cudaMemcpy2DAsync(V1, pitch, r1, pitch, row, H, cudaMemcpyDeviceToDevice, s));
+    // segments: about one wave of resident warps over all strips, at least 8 rows
+    const int nstrips = (W + kMpStrip - 1) / kMpStrip;
+    const long target = (long)sm_count() * kMpWarps * kMpBlocksPerSm;
+    const long nseg = std::max(1L, (target + nstrips - 1) / nstrips);
+    const int seg_rows = std::min(H, std::max(8, (int)((H + nseg - 1) / nseg)));
+    const int nitems = nstrips * ((H + seg_rows - 1) / seg_rows);
+    if (steps == 1) {  // V[0] = r only
+        if (V0 != r0) HS_CUDA_CHECK(cudaMemcpy2DAsync(V0, pitch, r0, pitch, row, H, cudaMemcpyDeviceToDevice, s));
+        if (V1 != r1) HS_CUDA_CHECK(cudaMemcpy2DAsync(V1, pitch, r1, pitch, row, H, cudaMemcpyDeviceToDevice, s));
+        return HS_OK;
+    }
     for (int s0 = 0; s0 + 1 < steps; s0 += depth) {
         const int d = std::min(depth, steps - 1 - s0);
-        float *b0 = V0 + (size_t)s0 * power_stride, *b1 = V1 + (size_t)s0 * power_stride;
+        MpParams pp;
+        pp.Ix = Ix;
+        pp.Iy = Iy;
+        pp.V0 = V0 + (size_t)s0 * power_stride;
+        pp.V1 = V1 + (size_t)s0 * power_stride;
+        // the first pass reads r itself and writes it out as V[0] (unless r is V[0])
+        pp.u_in = s0 == 0 ? r0 : pp.V0;
+        pp.v_in = s0 == 0 ? r1 : pp.V1;
+        pp.copy0 = (s0 == 0 && (V0 != r0 || V1 != r1)) ? 1 : 0;
+        pp.pstride = power_stride;
+        pp.H = H;
+        pp.W = W;
+        pp.ld = ld;
+        pp.seg_rows = seg_rows;
+        pp.nstrips = nstrips;
+        pp.nitems = nitems;
+        pp.lam = lam;
         switch (d) {  // this pass's depth
-            case 1: st = launch_mp<1>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
-            case 2: st = launch_mp<2>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
-            case 3: st = launch_mp<3>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
-            default: st = launch_mp<4>(lam, Ix, Iy, b0, b1, b0, b1, power_stride, H, W, ld, s); break;
+            case 1: st = launch_mp<1>(pp, s); break;
+            case 2: st = launch_mp<2>(pp, s); break;
+            case 3: st = launch_mp<3>(pp, s); break;
+            default: st = launch_mp<4>(pp, s); break;
         }
         if (st != HS_OK) return st;
     }

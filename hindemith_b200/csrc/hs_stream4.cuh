@@ -3,7 +3,7 @@
 //
 // Same pipeline as hs_stream.cuh (T sweeps per HBM pass as a register pipeline down the
 // strip, rolling 2-register windows per column-plane, a per-warp shared-memory ring fed
-// by cp.async, a ring of packed coefficients), with three differences that cut
+// by cp.async, a (T+1)-slot ring of packed coefficients), with three differences that cut
 // the instructions per cell-sweep:
 //   - a lane's 4 columns are one 16-byte chunk of each plane row, which the lane copies and
 //     reads itself: no lane reads another's copy, so no warp barrier brackets the copy;
@@ -29,23 +29,11 @@ constexpr int kWideCols = 128;        // columns per strip (4 per lane)
 constexpr int kWidePrefetch = 2;      // rows in flight per warp
 constexpr int kWideRawSlots = kWidePrefetch + 1;
 
-// Stage groups of the wide pipeline.  The T stages form G groups of consecutive stages
-// (group of stage s: g(s) = s G / T).  Inside a group a stage consumes the row its
-// predecessor emitted in the same step; the first stage of group g > 0 consumes the row
-// group g-1 emitted in the previous step.  Stage s therefore receives row k - s - g(s) at
-// step k, and the G groups of one step are independent dependency chains that the warp can
-// issue side by side.  Every stage still sees the same rows in the same order (only later),
-// so results do not depend on G; the cost is G-1 rows of lag (one more coefficient slot and
-// one held row of (u, v) per group boundary).
-constexpr int wide_groups(int T) { return 1; }
-constexpr int wgroup(int s, int T) { return s * wide_groups(T) / T; }
-
 template <int T>
 struct GeoW {
-    static constexpr int G = wide_groups(T);
     static constexpr int halo = (T + 3) & ~3;                  // 16-byte aligned lane chunks
     static constexpr int strip = kWideCols - 2 * halo;         // output columns per strip
-    static constexpr int coef_slots = T + G;                   // rows k-T-G+1 .. k
+    static constexpr int coef_slots = T + 1;                   // rows k-T .. k
     static constexpr int raw_floats = kWideRawSlots * kRawPlanes * kWideCols;
     static constexpr int coef_floats = coef_slots * 4 * 32 * 4;  // [slot][4][lane] float4
     static constexpr int warp_floats = raw_floats + coef_floats;
@@ -54,7 +42,7 @@ struct GeoW {
 
 struct ItemW {
     float *raw;     // [kWideRawSlots][kRawPlanes][128]
-    float4 *coef;   // [T+G][4][32]: per pair (0,2) then (1,3): (Ix, Iy) then (It, -1/den)
+    float4 *coef;   // [T+1][4][32]: per pair (0,2) then (1,3): (Ix, Iy) then (It, -1/den)
     int lane;
     int lcol;       // this lane's chunk, clamped to an in-bounds chunk of the row
     int xa;         // first of the lane's 4 columns
@@ -79,18 +67,16 @@ __device__ __forceinline__ void issue_row_w(const ItemW &it, int slot, int row, 
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
-// HEAD: one of the first 2T-2+G-1 steps of a segment that starts T or more rows below the
-// image top; stage s only runs from its segment step kk = k - k0 = 2s + g(s) on (see
-// stream_item_w).  `held` carries the rows the group boundaries pass to the next step.
+// HEAD: one of the first 2T-2 steps of a segment that starts T or more rows below the
+// image top; stage s only runs from its segment step kk = k - k0 = 2s on (see stream_item_w).
 // XE: 0 = no image side in the strip; 1 = a side, any W; 2 = a side with W % 4 == 0, where
 // column W-1 is always a lane's last column (chunks start at multiples of 4), so only the
 // first column's left clamp and the last column's right clamp can apply.
 // DUMP (the training recompute) also writes every stage's sweep to p.dump_u/v.
 template <int T, int XE, bool EDGE, bool HEAD = false, bool DUMP = false>
 __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW &it,
-                                              Win<true> (&w)[T][2][2],
-                                              float2 (&held)[GeoW<T>::G][2][2], int k, int rslot,
-                                              int cslot, int kk = 0) {
+                                              Win<true> (&w)[T][2][2], int k, int rslot, int cslot,
+                                              int kk = 0) {
     // prefetch row k + kWidePrefetch into the slot row k-1 used, then wait for row k; the
     // lane only ever reads its own copies
     issue_row_w(it, rslot == 0 ? kWideRawSlots - 1 : rslot - 1, min(k + kWidePrefetch, it.y_end - 1 + T), p);
@@ -112,32 +98,15 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
         cs[64] = make_float4(ix.y, ix.w, iy.y, iy.w);
         cs[96] = make_float4(t4.y, t4.w, n1, n3);
     }
-    constexpr int G = GeoW<T>::G;
     // [plane][pair]: pair 0 holds columns (0, 2), pair 1 columns (1, 3)
     float2 cu[2][2] = {{make_float2(u4.x, u4.z), make_float2(u4.y, u4.w)},
                        {make_float2(v4.x, v4.z), make_float2(v4.y, v4.w)}};
     const float2 we2 = make_float2(p.we, p.we), wc2 = make_float2(p.wc, p.wc);
-    // the rows the group boundaries hold for the next step: group g > 0 starts from the row
-    // group g-1 emitted last step (read here, before this step's emission replaces it)
-    float2 in_g[G][2][2];
-#pragma unroll
-    for (int g = 1; g < G; ++g)
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) in_g[g][a][b] = held[g][a][b];
 
 #pragma unroll
     for (int s = 0; s < T; ++s) {
-        const int g = wgroup(s, T);
-        if (HEAD && kk < 2 * s + g) continue;  // warp-uniform: the stage has no valid input yet
-        if (g > 0 && wgroup(s - 1, T) != g) {  // first stage of a later group
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) cu[a][b] = in_g[g][a][b];
-        }
-        const int n = k - s - g;  // arriving row (input of sweep s+1)
+        if (HEAD && kk < 2 * s) break;  // warp-uniform; later stages start later still
+        const int n = k - s;  // arriving row (input of sweep s+1)
         float2 ub[2][2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -159,7 +128,7 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             ub[q][0] = win_step<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
             ub[q][1] = win_step<EDGE>(w[s][q][1], E, O, rO, n, p.H, we2, wc2);
         }
-        int rs = cslot - (s + g + 1);
+        int rs = cslot - (s + 1);
         if (rs < 0) rs += GeoW<T>::coef_slots;
         const float4 *cr = it.coef + rs * 128 + it.lane;
 #pragma unroll
@@ -173,14 +142,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             cu[0][j] = fma2(cx, nt, ubar);
             cu[1][j] = fma2(cy, nt, vbar);
         }
-        if (s + 1 < T && wgroup(s + 1, T) != g) {  // last stage of a group: hold its row
-#pragma unroll
-            for (int a = 0; a < 2; ++a)
-#pragma unroll
-                for (int b = 0; b < 2; ++b) held[g + 1][a][b] = cu[a][b];
-        }
-        if constexpr (DUMP) {  // write sweep s+1 of row k-s-g-1 (state dumps)
-            const int rr = k - s - g - 1;
+        if constexpr (DUMP) {  // write sweep s+1 of row k-s-1 (state dumps)
+            const int rr = k - s - 1;
             if (rr >= it.y_start && rr < it.y_end) {
                 const size_t off = (size_t)rr * p.ld + it.xa;
                 const float du[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
@@ -200,9 +163,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
         }
     }
 
-    // store sweep T of row k - T - G + 1 (the last stage's row); a head step whose last
-    // stage did not run has no row to store (it lies above y_start)
-    const int r = k - T - G + 1;
+    // store sweep T of row k - T
+    const int r = k - T;
     if (r >= it.y_start && r < it.y_end) {
         const size_t off = (size_t)r * p.ld + it.xa;
         const float uo[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
@@ -223,9 +185,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
 
 template <int T, int XE, bool DUMP>
 __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW &it) {
-    constexpr int G = GeoW<T>::G;
     const int k0 = max(0, it.y_start - T);
-    const int k_end = it.y_end - 1 + T + G - 1;
+    const int k_end = it.y_end - 1 + T;
     Win<true> w[T][2][2];
 #pragma unroll
     for (int s = 0; s < T; ++s)
@@ -233,19 +194,12 @@ __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW 
         for (int q = 0; q < 2; ++q)
 #pragma unroll
             for (int j = 0; j < 2; ++j) w[s][q][j] = Win<true>{};
-    float2 held[G][2][2];
-#pragma unroll
-    for (int g = 0; g < G; ++g)
-#pragma unroll
-        for (int a = 0; a < 2; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) held[g][a][b] = make_float2(0.f, 0.f);
 
 #pragma unroll
     for (int i = 0; i < kWidePrefetch; ++i) issue_row_w(it, i, k0 + i, p);
 
     // steps in [klo, khi] have no stage at row 0 or past row H-2: no clamp logic
-    const int klo = max(k0, T + G - 1);
+    const int klo = max(k0, T);
     const int khi = min(k_end, p.H - 2);
     int k = k0, rslot = 0, cslot = 0;
     auto advance = [&]() {
@@ -254,26 +208,24 @@ __device__ __forceinline__ void stream_item_w(const SweepParams &p, const ItemW 
         cslot = (cslot + 1 == GeoW<T>::coef_slots) ? 0 : cslot + 1;
     };
     // A segment starting T or more rows below the top (k0 = y_start - T > 0) needs stage s's
-    // output only from row y_start - (T-1-s) = k0 + s + 1 on, which needs the rows it
-    // receives from row k0 + s on (stage s-1's first valid rows); stage s receives row
-    // k0 + s at segment step 2s + g(s).  Stage s therefore does nothing useful before that
-    // step: the first 2T-2+G-1 steps skip those stages, T(T-1) + sum g(s) stage-steps per
-    // segment.
-    constexpr int kHead = 2 * (T - 1) + G - 1;
-    if (!DUMP && k0 >= T && k0 + kHead <= khi) {  // (dump passes: as the 2-column kernel)
-        for (int kk = 0; kk < kHead; ++kk, advance())
-            stream_step_w<T, XE, false, true>(p, it, w, held, k, rslot, cslot, kk);
+    // output only from row y_start - (T-1-s) = k0 + s + 1 on, which it first emits at
+    // segment step 2s + 2, from the rows it receives at steps 2s and 2s + 1 (stage s-1's
+    // first valid rows).  Stage s therefore does nothing useful before step 2s: the first
+    // 2T-2 steps skip those stages, T(T-1) stage-steps per segment.
+    if (!DUMP && k0 >= T && k0 + 2 * T - 2 <= khi) {  // (dump passes: as the 2-column kernel)
+        for (int kk = 0; kk < 2 * T - 2; ++kk, advance())
+            stream_step_w<T, XE, false, true>(p, it, w, k, rslot, cslot, kk);
     }
     if (klo + 1 <= khi) {
-        for (; k < klo; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, held, k, rslot, cslot);
+        for (; k < klo; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, k, rslot, cslot);
         while (k + 1 <= khi) {
-            stream_step_w<T, XE, false, false, DUMP>(p, it, w, held, k, rslot, cslot);
+            stream_step_w<T, XE, false, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
-            stream_step_w<T, XE, false, false, DUMP>(p, it, w, held, k, rslot, cslot);
+            stream_step_w<T, XE, false, false, DUMP>(p, it, w, k, rslot, cslot);
             advance();
         }
     }
-    for (; k <= k_end; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, held, k, rslot, cslot);
+    for (; k <= k_end; advance()) stream_step_w<T, XE, true, false, DUMP>(p, it, w, k, rslot, cslot);
     cp_async_wait<0>();
 }
 

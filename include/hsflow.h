@@ -275,7 +275,7 @@ HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *
  * in the template's operation order (bit-identical to its FP32 semantics).  V0, V1 hold
  * `steps` planes each, power s at V + s * power_stride floats (power_stride >= H*ld, a
  * multiple of 4).  cfg->sweeps_per_pass (1..4, 0 = 4) powers are computed per pass over
- * HBM from one shared-memory tile. */
+ * HBM, streaming the image in column strips with the powers as a register pipeline. */
 HS_API hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const float *r0,
                                   const float *r1, int H, int W, int ld, int steps, float *V0,
                                   float *V1, size_t power_stride, const hs_config *cfg,

@@ -2,7 +2,7 @@
 that holds the reference checkout; the fixtures are committed, this script is not run
 by the tests).
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 
 The reference's only CPU implementation of the path is its NumPy library, hlib.py
 (Stencil.__mul__ at hlib.py:173-191, warp_img2d at hlib.py:120-138).  It is Python 2
@@ -201,4 +201,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path of the reference checkout>")
+    main(sys.argv[1])

@@ -35,6 +35,35 @@ def test_matrix_powers_bitexact(cuda, shape, depth):
         assert_bitexact(V1[s].cpu().numpy(), R1[s], f"V1[{s}]")
 
 
+@pytest.mark.parametrize("depth", [3, 4])
+def test_matrix_powers_large_and_in_place(cuda, depth):
+    """Many strips and segments (1000x1500, ld padded), and V[0] given as r itself: the
+    powers still equal the FP32 restatement bit for bit."""
+    import ctypes
+
+    from hindemith_b200 import device as D
+
+    H, W, steps = 1000, 1498, 9
+    rng = np.random.default_rng(depth)
+    Ix, Iy, r0, r1 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(4))
+    lam = np.float32(0.4)
+    R0, R1 = O.c_hs_matrix_powers(lam, Ix, Iy, r0, r1, steps)
+    Ixd, Iyd = D.as_plane(cuda32(Ix)), D.as_plane(cuda32(Iy))
+    ld = D.ld_of(Ixd)
+    buf = torch.empty((2, steps, H, ld), dtype=torch.float32, device="cuda")
+    buf[0, 0, :, :W] = cuda32(r0)
+    buf[1, 0, :, :W] = cuda32(r1)
+    cfg = L.make_config(sweeps_per_pass=depth)
+    L.check(L.lib().hs_matrix_powers(float(lam), D.ptr(Ixd), D.ptr(Iyd), D.ptr(buf[0, 0]),
+                                     D.ptr(buf[1, 0]), H, W, ld, steps, D.ptr(buf[0, 0]),
+                                     D.ptr(buf[1, 0]), H * ld, ctypes.byref(cfg),
+                                     D.stream_handle()), "hs_matrix_powers")
+    torch.cuda.synchronize()
+    for s in range(steps):
+        assert_bitexact(buf[0, s, :, :W].cpu().numpy(), R0[s], f"V0[{s}]")
+        assert_bitexact(buf[1, s, :, :W].cpu().numpy(), R1[s], f"V1[{s}]")
+
+
 def test_matrix_powers_single_step_is_copy(cuda):
     rng = np.random.default_rng(1)
     a = [rng.standard_normal((9, 11)).astype(np.float32) for _ in range(4)]
