@@ -129,8 +129,8 @@ def clear():
 
 # (T, rows per tile, layout): 1 = 2 columns per lane, 2 = 4 (fast form only)
 BATCH_CANDIDATES = ((3, 96, 1), (4, 64, 1), (4, 96, 1), (5, 96, 1), (5, 128, 1), (6, 128, 1),
-                    (6, 96, 1), (6, 128, 2), (6, 96, 2), (5, 128, 2), (5, 96, 2), (5, 64, 2),
-                    (4, 128, 2), (4, 96, 2))
+                    (6, 96, 1), (6, 128, 2), (6, 96, 2), (6, 192, 2), (5, 128, 2), (5, 96, 2),
+                    (5, 64, 2), (5, 160, 2), (5, 192, 2), (4, 128, 2), (4, 96, 2), (4, 192, 2))
 
 
 def _log(entry):

@@ -801,60 +801,59 @@ static hs_status train_backward(const hs_train_pair *pairs, const PairBufs *bufs
         }
         return HS_OK;
     };
-    // 2. adjoint sweeps j = nsw-1 .. 0 of interval b in ceil(nsw / TB) passes of balanced
-    //    depth (10 = 4 + 3 + 3)
-    auto adjoint = [&](int b) -> hs_status {
-        const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
-        const int sb = b & 1;
-        const int npass = (nsw + TB - 1) / TB;
-        for (int jhi = nsw, q = 0; jhi > 0; ++q) {
-            const int tb = (jhi + (npass - q) - 1) / (npass - q);
-            AdjTable tab;
-            memset(&tab, 0, sizeof(tab));
-            tab.npairs = n;
-            tab.we = rc.we;
-            tab.wc = rc.wc;
-            long rows = 0;
-            for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
-            const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
-            int Lr = (int)std::max(1L, (rows + target - 1) / target);
-            Lr = std::max(Lr, std::max(8, 2 * tb));
-            tab.item_prefix[0] = 0;
-            for (int i = 0; i < n; ++i) {
-                const hs_train_pair &d = pairs[i];
-                const PairBufs &B = bufs[i];
-                AdjPair &P = tab.pair[i];
-                P.Ix = B.deriv(0);
-                P.Iy = B.deriv(1);
-                P.It = B.deriv(2);
-                P.lu_in = B.lamb(cur, 0);
-                P.lv_in = B.lamb(cur, 1);
-                P.lu_out = B.lamb(cur ^ 1, 0);
-                P.lv_out = B.lamb(cur ^ 1, 1);
-                for (int qq = 0; qq < tb; ++qq) {
-                    const int j = jhi - qq;  // x_{k_lo + j}
-                    P.xu[qq] = (j == nsw) ? B.ck(b + 1, 0) : B.state(j, 0, sb);
-                    P.xv[qq] = (j == nsw) ? B.ck(b + 1, 1) : B.state(j, 1, sb);
-                }
-                P.aIx = B.accum(0);
-                P.aIy = B.accum(1);
-                P.aIt = B.accum(2);
-                P.a2part = B.a2part;
-                P.alpha_dev = d.alpha;
-                P.H = d.H;
-                P.W = d.W;
-                P.ld = d.ld;
-                P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
-                P.seg_rows = std::min(Lr, d.H);
-                const int items = P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
-                if (items > nslots) HS_FAIL(HS_ERR_INVALID_ARG, "adjoint items %d > slots %d", items, nslots);
-                tab.item_prefix[i + 1] = tab.item_prefix[i] + items;
+    // 2. the adjoint sweeps m = iters .. 1 in ceil(iters / TB) passes of balanced depth
+    //    (200 = 50 x 4).  A pass may span two checkpoint intervals: x_m is checkpoint
+    //    m / k when k divides m (or m = iters), else state m - b k of interval b = (m-1)/k.
+    auto interval_of = [&](int m) { return (m - 1) / ckpt_every; };
+    auto nsw_of = [&](int b) { return std::min(ckpt_every, iters - b * ckpt_every); };
+    auto state_ptr = [&](const PairBufs &B, int m, int comp) -> const float * {
+        const int b = interval_of(m), j = m - b * ckpt_every;
+        return j == nsw_of(b) ? B.ck(b + 1, comp) : B.state(j, comp, b & 1);
+    };
+    auto adjoint_pass = [&](int jhi, int tb, cudaStream_t as) -> hs_status {
+        AdjTable tab;
+        memset(&tab, 0, sizeof(tab));
+        tab.npairs = n;
+        tab.we = rc.we;
+        tab.wc = rc.wc;
+        long rows = 0;
+        for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
+        const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
+        int Lr = (int)std::max(1L, (rows + target - 1) / target);
+        Lr = std::max(Lr, std::max(8, 2 * tb));
+        tab.item_prefix[0] = 0;
+        for (int i = 0; i < n; ++i) {
+            const hs_train_pair &d = pairs[i];
+            const PairBufs &B = bufs[i];
+            AdjPair &P = tab.pair[i];
+            P.Ix = B.deriv(0);
+            P.Iy = B.deriv(1);
+            P.It = B.deriv(2);
+            P.lu_in = B.lamb(cur, 0);
+            P.lv_in = B.lamb(cur, 1);
+            P.lu_out = B.lamb(cur ^ 1, 0);
+            P.lv_out = B.lamb(cur ^ 1, 1);
+            for (int qq = 0; qq < tb; ++qq) {  // stage qq reverses sweep jhi - qq
+                P.xu[qq] = state_ptr(B, jhi - qq, 0);
+                P.xv[qq] = state_ptr(B, jhi - qq, 1);
             }
-            hs_status e = launch_adj_any(tb, tab, s);
-            if (e != HS_OK) return e;
-            cur ^= 1;
-            jhi -= tb;
+            P.aIx = B.accum(0);
+            P.aIy = B.accum(1);
+            P.aIt = B.accum(2);
+            P.a2part = B.a2part;
+            P.alpha_dev = d.alpha;
+            P.H = d.H;
+            P.W = d.W;
+            P.ld = d.ld;
+            P.nstrips = (d.W + strip_cols_for(tb) - 1) / strip_cols_for(tb);
+            P.seg_rows = std::min(Lr, d.H);
+            const int items = P.nstrips * ((d.H + P.seg_rows - 1) / P.seg_rows);
+            if (items > nslots) HS_FAIL(HS_ERR_INVALID_ARG, "adjoint items %d > slots %d", items, nslots);
+            tab.item_prefix[i + 1] = tab.item_prefix[i] + items;
         }
+        hs_status e = launch_adj_any(tb, tab, as);
+        if (e != HS_OK) return e;
+        cur ^= 1;
         return HS_OK;
     };
 
@@ -869,27 +868,58 @@ static hs_status train_backward(const hs_train_pair *pairs, const PairBufs *bufs
     } else {
         lock.unlock();
     }
-    if (!S) {
-        for (int b = nb - 1; b >= 0; --b) {
-            if ((st = dump(b, s)) != HS_OK) return st;
-            if ((st = adjoint(b)) != HS_OK) return st;
-        }
-    } else {
+    // Schedule.  Interval b's states are recomputed (dump) before the first pass that reads
+    // them; its buffer (parity b & 1) is free again once the last pass reading interval
+    // b+2 has run.  With the side stream the recompute runs up to two intervals ahead of the
+    // passes: dump(b) waits for the passes of b+2 to finish (event adj_done[b & 1]) and the
+    // passes reading b wait for dump(b) (event dump_done[b & 1]).
+    const cudaStream_t ds = S ? S->s : s;
+    int next_dump = nb - 1;  // intervals >= next_dump have their dump issued
+    auto issue_dump = [&](int b) -> hs_status {
+        if (S && b + 2 <= nb - 1) HS_CUDA_CHECK(cudaStreamWaitEvent(ds, S->adj_done[b & 1], 0));
+        hs_status e = dump(b, ds);
+        if (e != HS_OK) return e;
+        if (S) HS_CUDA_CHECK(cudaEventRecord(S->dump_done[b & 1], ds));
+        next_dump = b - 1;
+        return HS_OK;
+    };
+    if (S) {
         // the side stream starts after everything the caller queued before this call
         HS_CUDA_CHECK(cudaEventRecord(S->start, s));
-        HS_CUDA_CHECK(cudaStreamWaitEvent(S->s, S->start, 0));
-        if ((st = dump(nb - 1, S->s)) != HS_OK) return st;
-        HS_CUDA_CHECK(cudaEventRecord(S->dump_done[(nb - 1) & 1], S->s));
-        for (int b = nb - 1; b >= 0; --b) {
-            if (b >= 1) {  // recompute b-1 into buffer (b-1) & 1, last read by adjoint(b+1)
-                if (b + 1 <= nb - 1) HS_CUDA_CHECK(cudaStreamWaitEvent(S->s, S->adj_done[(b + 1) & 1], 0));
-                if ((st = dump(b - 1, S->s)) != HS_OK) return st;
+        HS_CUDA_CHECK(cudaStreamWaitEvent(ds, S->start, 0));
+        if ((st = issue_dump(nb - 1)) != HS_OK) return st;
+        if (nb >= 2 && (st = issue_dump(nb - 2)) != HS_OK) return st;
+    }
+    const int npass = (iters + TB - 1) / TB;
+    for (int jhi = iters, q = 0; jhi > 0; ++q) {
+        const int tb = (jhi + (npass - q) - 1) / (npass - q);
+        const int jlo = jhi - tb + 1;
+        const int b_hi = interval_of(jhi), b_lo = interval_of(jlo);
+        // the recompute of every interval whose states this pass reads (at most two adjacent
+        // intervals for depth <= 4 and k >= 2; none for k = 1); in order without a side stream
+        for (int b = b_hi; b >= b_lo; --b) {
+            bool reads = false;
+            for (int m = jlo; m <= jhi; ++m)
+                reads |= interval_of(m) == b && m - b * ckpt_every != nsw_of(b);
+            if (!reads) continue;
+            if (!S) {
+                while (next_dump >= b)
+                    if ((st = issue_dump(next_dump)) != HS_OK) return st;
+            } else {
+                if (next_dump >= b) HS_FAIL(HS_ERR_INVALID_ARG, "internal: interval %d read before its recompute", b);
+                HS_CUDA_CHECK(cudaStreamWaitEvent(s, S->dump_done[b & 1], 0));
             }
-            HS_CUDA_CHECK(cudaStreamWaitEvent(s, S->dump_done[b & 1], 0));
-            if (b >= 1) HS_CUDA_CHECK(cudaEventRecord(S->dump_done[(b - 1) & 1], S->s));
-            if ((st = adjoint(b)) != HS_OK) return st;
-            HS_CUDA_CHECK(cudaEventRecord(S->adj_done[b & 1], s));
         }
+        if ((st = adjoint_pass(jhi, tb, s)) != HS_OK) return st;
+        // intervals no later pass reads: above b_lo, and b_lo itself once its first sweep is
+        // reversed; their buffers go to the recompute two intervals further down
+        const int b_done_lo = (jlo == b_lo * ckpt_every + 1) ? b_lo : b_lo + 1;
+        for (int b = b_hi; b >= b_done_lo; --b) {
+            if (!S) continue;
+            HS_CUDA_CHECK(cudaEventRecord(S->adj_done[b & 1], s));
+            if (b - 2 >= 0 && next_dump == b - 2 && (st = issue_dump(b - 2)) != HS_OK) return st;
+        }
+        jhi -= tb;
     }
 
     // 3. transposed derivative stencils and dalpha
