@@ -223,9 +223,12 @@ HS_API hs_status hs_forward_train_batched(const hs_train_pair *pairs, int n, int
                                           const hs_config *cfg, void *stream);
 
 /* Backward of the preceding hs_forward_train_batched (same pairs, iters, ckpt_every and
- * workspace): per checkpoint interval, the states are recomputed by dump passes (each
- * stage of a T-sweep pass writes its state) and the adjoint runs temporally blocked,
- * sweeps_per_pass (at most 5) adjoint sweeps per HBM pass.  Needs alpha != 0. */
+ * workspace): each checkpoint interval's states are recomputed by dump passes (each stage
+ * of a T-sweep pass writes its state), on a library-owned side stream up to two intervals
+ * ahead, and the adjoint runs temporally blocked on the caller's stream, min(4,
+ * sweeps_per_pass) adjoint sweeps per HBM pass in passes of balanced depth that may span
+ * two intervals.  The side stream joins a capture of the caller's stream through events and
+ * is joined back before the call returns.  Needs alpha != 0.  Deterministic. */
 HS_API hs_status hs_backward_batched(const hs_train_pair *pairs, int n, int iters, int ckpt_every,
                                      void *workspace, size_t workspace_bytes,
                                      const hs_config *cfg, void *stream);
