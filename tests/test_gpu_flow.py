@@ -31,6 +31,18 @@ def test_lk_bitexact(cuda, shape, rad):
     assert_bitexact(dv.cpu().numpy(), rdv)
 
 
+def test_lk_against_reference_template_golden(cuda):
+    """hs_lk_least_squares against the reference's LKLeastSquares device template run as C
+    (tests/golden/make_lk_golden.py): bit-identical."""
+    g = golden("lk.npz")
+    for i in range(int(g["n"])):
+        du, dv = FL.lk_least_squares(cuda32(g[f"err_{i}"]), cuda32(g[f"Ix_{i}"]), cuda32(g[f"Iy_{i}"]),
+                                     int(g[f"rad_{i}"]))
+        torch.cuda.synchronize()
+        assert_bitexact(du.cpu().numpy(), g[f"du_{i}"], f"case {i}")
+        assert_bitexact(dv.cpu().numpy(), g[f"dv_{i}"], f"case {i}")
+
+
 def test_brox_against_reference_golden(cuda):
     g = golden("brox.npz")
     offx, offy = brox_offsets()

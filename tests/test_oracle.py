@@ -248,10 +248,21 @@ def test_brox_oracle_matches_reference_golden():
         assert_bitexact(y1, g[f"y1_{i}"])
 
 
+def test_lk_oracle_matches_reference_template_golden():
+    """The LKLeastSquares restatement against the reference's own device template
+    (LKLeastSquares.cpp:39-91), instantiated as C by tests/golden/make_lk_golden.py:
+    bit-identical, including the border rule and det == 0 windows."""
+    g = golden("lk.npz")
+    for i in range(int(g["n"])):
+        du, dv = O.c_lk_least_squares(g[f"err_{i}"], g[f"Ix_{i}"], g[f"Iy_{i}"], int(g[f"rad_{i}"]))
+        assert_bitexact(du, g[f"du_{i}"], f"case {i}")
+        assert_bitexact(dv, g[f"dv_{i}"], f"case {i}")
+
+
 def test_lk_oracle_matches_float64_restatement():
     """The LKLeastSquares restatement against an independent FP64 NumPy evaluation of the
-    same template (window [-r, r)^2, interior rule): parity unpinned against the reference
-    itself, whose NumPy lk_least_squares (hlib.py:86-118) uses a (2r+1)^2 window."""
+    same template (window [-r, r)^2, interior rule).  (The reference's NumPy
+    lk_least_squares, hlib.py:86-118, is a different algorithm with a (2r+1)^2 window.)"""
     rng = np.random.default_rng(9)
     for (H, W, r) in ((12, 15, 2), (20, 9, 3), (5, 5, 2)):
         err, Ix, Iy = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(3))
