@@ -126,8 +126,14 @@ __global__ void __launch_bounds__(256) upsample2_adjoint_kernel(const float *__r
 
 // WarpImg2D.cpp:33-75: the integer part truncates toward zero, then steps down for a
 // negative offset; the fraction is a float; a pixel whose 2x2 footprint leaves the image
-// keeps the source value.  As in the OpenCL template the weights are formed in double and
-// each of the four accumulations rounds to the float output.
+// keeps the source value.  The four accumulations follow C's (and OpenCL C's) typing of
+// the template's expressions, evaluated left to right: a product stays float until a
+// double operand (1.0 - frac) joins it, and an accumulation whose term is double rounds
+// the double sum to the float output:
+//   o  = float(0 + src00 * (1.0 - xf) * (1.0 - yf))          all double
+//   o  = float(o + float(src10 * xf) * (1.0 - yf))           float product, then double
+//   o  = float(o + src01 * (1.0 - xf) * yf)                  all double
+//   o  = o + float(float(src11 * xf) * yf)                    all float
 __global__ void __launch_bounds__(256) warp_kernel(const float *__restrict__ src,
                                                    const float *__restrict__ ou,
                                                    const float *__restrict__ ov, int H, int W,
@@ -147,14 +153,14 @@ __global__ void __launch_bounds__(256) warp_kernel(const float *__restrict__ src
     float o;
     if (x + mx >= 0 && x + mx + 1 < W && y + my >= 0 && y + my + 1 < H) {
         const size_t b = (size_t)(x + mx) + (size_t)(y + my) * ld;
-        // explicit roundings: no double FMA contraction, products left to right
+        // explicit roundings: no FMA contraction, products left to right
         const double xd = xfrac, yd = yfrac;
         const double nx = __dsub_rn(1.0, xd), ny = __dsub_rn(1.0, yd);
         o = 0.0f;
         o = (float)__dadd_rn(o, __dmul_rn(__dmul_rn(__ldg(src + b), nx), ny));
-        o = (float)__dadd_rn(o, __dmul_rn(__dmul_rn(__ldg(src + b + 1), xd), ny));
+        o = (float)__dadd_rn(o, __dmul_rn((double)__fmul_rn(__ldg(src + b + 1), xfrac), ny));
         o = (float)__dadd_rn(o, __dmul_rn(__dmul_rn(__ldg(src + b + ld), nx), yd));
-        o = (float)__dadd_rn(o, __dmul_rn(__dmul_rn(__ldg(src + b + ld + 1), xd), yd));
+        o = __fadd_rn(o, __fmul_rn(__fmul_rn(__ldg(src + b + ld + 1), xfrac), yfrac));
     } else {
         o = __ldg(src + i);
     }

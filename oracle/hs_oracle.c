@@ -310,11 +310,13 @@ HSO_API int hso_hs_forward_f64(const double *I0, const double *I1, int H, int W,
 
 /* WarpImg2D.cpp:33-75: backward bilinear warp of src by the offsets (ox, oy).  The
  * integer part truncates toward zero and is then floored for negative offsets; a
- * pixel whose 2x2 footprint leaves the image keeps the source value.  In OpenCL C
- * the template's `1.0` literals are double: `xfrac = 1.0 + xfrac` rounds back to the
- * float variable, and each `OUT += IN * (1.0 - xfrac) * (1.0 - yfrac)` forms its
- * product in double and rounds the sum to the float output.  This restatement keeps
- * exactly those roundings. */
+ * pixel whose 2x2 footprint leaves the image keeps the source value.  In OpenCL C, as
+ * in C, the template's `1.0` literals are double and each expression is typed left to
+ * right: `xfrac = 1.0 + xfrac` rounds back to the float variable; `IN * (1.0 - xfrac) *
+ * (1.0 - yfrac)` is double throughout, `IN * (xfrac) * (1.0 - yfrac)` rounds the float
+ * product IN * xfrac before the double one, and `IN * (xfrac) * (yfrac)` is all float;
+ * `OUT += term` rounds a double sum to the float output, or adds in float for the float
+ * term.  This restatement keeps exactly those roundings. */
 HSO_API void hso_warp_f32(const float *src, const float *ox, const float *oy, int H, int W,
                           float *dst) {
 #pragma omp parallel for schedule(static)
@@ -328,12 +330,13 @@ HSO_API void hso_warp_f32(const float *src, const float *ox, const float *oy, in
             if (fy < 0.0) { my--; yfrac = (float)(1.0 + (double)yfrac); }
             if (x + mx >= 0 && x + mx + 1 < W && y + my >= 0 && y + my + 1 < H) {
                 size_t b = (size_t)(x + mx) + (size_t)(y + my) * W;
-                double xd = xfrac, yd = yfrac;
+                /* C's typing of the template's expressions, left to right: float products
+                 * until (1.0 - frac) makes them double */
                 float o = 0.0f;
-                o = (float)((double)o + (double)src[b] * (1.0 - xd) * (1.0 - yd));
-                o = (float)((double)o + (double)src[b + 1] * xd * (1.0 - yd));
-                o = (float)((double)o + (double)src[b + W] * (1.0 - xd) * yd);
-                o = (float)((double)o + (double)src[b + W + 1] * xd * yd);
+                o = (float)((double)o + (double)src[b] * (1.0 - xfrac) * (1.0 - yfrac));
+                o = (float)((double)o + (double)(src[b + 1] * xfrac) * (1.0 - yfrac));
+                o = (float)((double)o + (double)src[b + W] * (1.0 - xfrac) * (double)yfrac);
+                o = o + src[b + W + 1] * xfrac * yfrac;
                 dst[i] = o;
             } else {
                 dst[i] = src[i];

@@ -138,11 +138,13 @@ def warp(src, ox, oy):
     xd = xf.astype(np.float64)
     yd = yf.astype(np.float64)
     s = src.astype(np.float64)
+    # C's typing of the template's expressions, left to right: float products until
+    # (1.0 - frac) makes them double
     o = np.zeros((H, W), dtype=np.float32)
     o = (o + s[by, bx] * (1.0 - xd) * (1.0 - yd)).astype(np.float32)
-    o = (o + s[by, bx1] * xd * (1.0 - yd)).astype(np.float32)
+    o = (o + (src[by, bx1] * xf).astype(np.float64) * (1.0 - yd)).astype(np.float32)
     o = (o + s[by1, bx] * (1.0 - xd) * yd).astype(np.float32)
-    o = (o + s[by1, bx1] * xd * yd).astype(np.float32)
+    o = o + (src[by1, bx1] * xf) * yf
     return np.where(ok, o, src).astype(np.float32)
 
 

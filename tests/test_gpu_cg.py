@@ -17,6 +17,21 @@ def cuda32(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).cuda()
 
 
+@pytest.mark.parametrize("depth", [1, 3, 4])
+def test_matrix_powers_against_reference_template_golden(cuda, depth):
+    """hs_matrix_powers against the reference's HSMatrixPowers device template run as C
+    (copy into plane 0, one launch per step): bit-identical at every pass depth."""
+    g = golden("matrix_powers.npz")
+    for i in range(int(g["n"])):
+        steps = int(g[f"steps_{i}"])
+        V0, V1 = cg.hs_matrix_powers(float(g[f"lam_{i}"]), *(cuda32(g[f"{k}_{i}"]) for k in ("Ix", "Iy", "r0", "r1")),
+                                     steps, L.make_config(sweeps_per_pass=depth))
+        torch.cuda.synchronize()
+        for s in range(steps):
+            assert_bitexact(V0[s].cpu().numpy(), g[f"V0_{i}"][s], f"case {i} V0[{s}]")
+            assert_bitexact(V1[s].cpu().numpy(), g[f"V1_{i}"][s], f"case {i} V1[{s}]")
+
+
 @pytest.mark.parametrize("shape", [(1, 1), (1, 5), (6, 1), (2, 3), (33, 65), (100, 130), (257, 96),
                                    (150, 250), (300, 517)])  # the last two have interior tiles
 @pytest.mark.parametrize("depth", [1, 2, 3, 4])

@@ -33,7 +33,7 @@ def test_lk_bitexact(cuda, shape, rad):
 
 def test_lk_against_reference_template_golden(cuda):
     """hs_lk_least_squares against the reference's LKLeastSquares device template run as C
-    (tests/golden/make_lk_golden.py): bit-identical."""
+    (tests/golden/make_template_golden.py): bit-identical."""
     g = golden("lk.npz")
     for i in range(int(g["n"])):
         du, dv = FL.lk_least_squares(cuda32(g[f"err_{i}"]), cuda32(g[f"Ix_{i}"]), cuda32(g[f"Iy_{i}"]),

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 import torch
 
+from conftest import golden
 from hindemith_b200 import _lib as L
 from hindemith_b200 import pyramid as PY
 from hindemith_b200 import synthetic
@@ -81,6 +82,15 @@ def test_warp_bitexact(cuda, shape, amp):
     torch.cuda.synchronize()
     ref = O.c_warp(src, ox, oy)
     np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+def test_warp_against_reference_template_golden(cuda):
+    """hs_warp against the reference's WarpImg2D device template run as C: bit-identical."""
+    g = golden("warp_template.npz")
+    for i in range(int(g["n"])):
+        out = PY.warp(cuda32(g[f"src_{i}"]), cuda32(g[f"ox_{i}"]), cuda32(g[f"oy_{i}"]))
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(out.cpu().numpy().view(np.uint32), g[f"out_{i}"].view(np.uint32))
 
 
 def test_warp_adjoint(cuda):

@@ -53,6 +53,28 @@ def test_warp_golden():
             np.testing.assert_array_equal(out[device_rule], src[device_rule])
 
 
+def test_warp_matches_reference_template_golden():
+    """Fractional offsets (integer, -0 and tiny negative ones among them) against the
+    reference's WarpImg2D device template run as C (tests/golden/make_template_golden.py):
+    both restatements bit-identical, C's left-to-right float/double typing included."""
+    g = golden("warp_template.npz")
+    for i in range(int(g["n"])):
+        src, ox, oy = g[f"src_{i}"], g[f"ox_{i}"], g[f"oy_{i}"]
+        assert_bitexact(O.c_warp(src, ox, oy), g[f"out_{i}"], f"C, case {i}")
+        assert_bitexact(O.warp(src, ox, oy), g[f"out_{i}"], f"NumPy, case {i}")
+
+
+def test_matrix_powers_matches_reference_template_golden():
+    """HSMatrixPowers' device template (copy into plane 0, one launch per step) run as C
+    (tests/golden/make_template_golden.py) against the C restatement: bit-identical."""
+    g = golden("matrix_powers.npz")
+    for i in range(int(g["n"])):
+        V0, V1 = O.c_hs_matrix_powers(g[f"lam_{i}"], g[f"Ix_{i}"], g[f"Iy_{i}"], g[f"r0_{i}"],
+                                      g[f"r1_{i}"], int(g[f"steps_{i}"]))
+        assert_bitexact(V0, g[f"V0_{i}"], f"V0, case {i}")
+        assert_bitexact(V1, g[f"V1_{i}"], f"V1, case {i}")
+
+
 def test_warp_fractional_numpy_vs_c():
     rng = np.random.default_rng(3)
     src = rng.random((23, 29), dtype=np.float32)
@@ -250,7 +272,7 @@ def test_brox_oracle_matches_reference_golden():
 
 def test_lk_oracle_matches_reference_template_golden():
     """The LKLeastSquares restatement against the reference's own device template
-    (LKLeastSquares.cpp:39-91), instantiated as C by tests/golden/make_lk_golden.py:
+    (LKLeastSquares.cpp:39-91), instantiated as C by tests/golden/make_template_golden.py:
     bit-identical, including the border rule and det == 0 windows."""
     g = golden("lk.npz")
     for i in range(int(g["n"])):
