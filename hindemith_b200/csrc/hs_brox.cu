@@ -217,7 +217,7 @@ __global__ void __launch_bounds__(256) brox_precond_kernel(const float *__restri
     const float a = __fadd_rn(__ldg(diag0 + i), m), d = __fadd_rn(__ldg(diag1 + i), m);
     const float b = __ldg(offdiag + i), e = __ldg(x0 + i), f = __ldg(x1 + i);
     const float det = __fsub_rn(__fmul_rn(a, d), __fmul_rn(b, b));
-    if (fabsf(det) > 1e-4f) {
+    if ((double)fabsf(det) > 1e-4) {  // the template's double comparison
         y0[i] = __fdiv_rn(__fsub_rn(__fmul_rn(e, d), __fmul_rn(b, f)), det);
         y1[i] = __fdiv_rn(__fadd_rn(__fmul_rn(-b, e), __fmul_rn(a, f)), det);
     } else {

@@ -202,7 +202,8 @@ __device__ __forceinline__ void precond_px(float s2, float a, float d, float b, 
     if (x > 0) { a = __fadd_rn(a, s2); d = __fadd_rn(d, s2); }
     if (y > 0) { a = __fadd_rn(a, s2); d = __fadd_rn(d, s2); }
     const float det = __fsub_rn(__fmul_rn(a, d), __fmul_rn(b, b));
-    if (fabsf(det) > 1e-15f) {
+    // the template's fabs(det) > 1e-15 compares in double: float(1e-15) lies above 1e-15
+    if ((double)fabsf(det) > 1e-15) {
         o0 = __fdiv_rn(__fsub_rn(__fmul_rn(e, d), __fmul_rn(b, f)), det);
         o1 = __fdiv_rn(__fadd_rn(__fmul_rn(-b, e), __fmul_rn(a, f)), det);
     } else {

@@ -400,7 +400,7 @@ HSO_API void hso_apply_hs_precond_f32(float s2, const float *diag0, const float 
             if (y > 0) { a += s2; d += s2; }
             const float b = offdiag[i], c = offdiag[i], e = x0[i], f = x1[i];
             const float det = a * d - b * c;
-            if (fabsf(det) > 1e-15f) {
+            if ((double)fabsf(det) > 1e-15) { /* the template compares in double */
                 y0[i] = (e * d - b * f) / det;
                 y1[i] = (-c * e + a * f) / det;
             } else {
@@ -508,7 +508,7 @@ HSO_API void hso_apply_brox_precond_f32(const float *mid, const float *diag0, co
             const float a = diag0[i] + mid[i], d = diag1[i] + mid[i];
             const float b = offdiag[i], c = offdiag[i], e = x0[i], f = x1[i];
             const float det = a * d - b * c;
-            if (fabsf(det) > 1e-4f) {
+            if ((double)fabsf(det) > 1e-4) { /* the template compares in double */
                 y0[i] = (e * d - b * f) / det;
                 y1[i] = (-c * e + a * f) / det;
             } else {

@@ -21,7 +21,7 @@ def cuda32(a):
 def test_matrix_powers_against_reference_template_golden(cuda, depth):
     """hs_matrix_powers against the reference's HSMatrixPowers device template run as C
     (copy into plane 0, one launch per step): bit-identical at every pass depth."""
-    g = golden("matrix_powers.npz")
+    g = golden("tmpl_matrix_powers.npz")
     for i in range(int(g["n"])):
         steps = int(g[f"steps_{i}"])
         V0, V1 = cg.hs_matrix_powers(float(g[f"lam_{i}"]), *(cuda32(g[f"{k}_{i}"]) for k in ("Ix", "Iy", "r0", "r1")),
@@ -96,6 +96,17 @@ def test_preconditioner_reference_golden(cuda, name):
         torch.cuda.synchronize()
         assert_bitexact(y0.cpu().numpy(), g[f"y0_{i}"])
         assert_bitexact(y1.cpu().numpy(), g[f"y1_{i}"])
+
+
+def test_preconditioner_against_reference_template_golden(cuda):
+    """ApplyHSPreconditioner's device template run as C, with determinants at, just below and
+    at minus float(1e-15) (compared in double, as the template does): bit-identical."""
+    g = golden("tmpl_precond.npz")
+    for i in range(int(g["n"])):
+        y0, y1 = cg.apply_hs_preconditioner(float(g[f"s2_{i}"]), *(cuda32(g[f"{k}_{i}"]) for k in ("d0", "d1", "od", "x0", "x1")))
+        torch.cuda.synchronize()
+        assert_bitexact(y0.cpu().numpy(), g[f"y0_{i}"], f"case {i}")
+        assert_bitexact(y1.cpu().numpy(), g[f"y1_{i}"], f"case {i}")
 
 
 def test_preconditioner_bitexact_with_singular_blocks(cuda):

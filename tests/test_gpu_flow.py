@@ -34,7 +34,7 @@ def test_lk_bitexact(cuda, shape, rad):
 def test_lk_against_reference_template_golden(cuda):
     """hs_lk_least_squares against the reference's LKLeastSquares device template run as C
     (tests/golden/make_template_golden.py): bit-identical."""
-    g = golden("lk.npz")
+    g = golden("tmpl_lk.npz")
     for i in range(int(g["n"])):
         du, dv = FL.lk_least_squares(cuda32(g[f"err_{i}"]), cuda32(g[f"Ix_{i}"]), cuda32(g[f"Iy_{i}"]),
                                      int(g[f"rad_{i}"]))
@@ -56,6 +56,29 @@ def test_brox_against_reference_golden(cuda):
         assert_bitexact(ax.cpu().numpy(), g[f"ax_{i}"])
         assert_bitexact(y0.cpu().numpy(), g[f"y0_{i}"])
         assert_bitexact(y1.cpu().numpy(), g[f"y1_{i}"])
+
+
+def test_brox_against_reference_template_golden(cuda):
+    """SetBroxMatrix, SetBroxRedblackMatrix, SpmvDIA2D and ApplyBroxPreconditioner against
+    their device templates run as C: bit-identical (matrices start from random values)."""
+    g = golden("tmpl_brox.npz")
+    offx, offy = brox_offsets()
+    for i in range(int(g["n"])):
+        A = FL.DeviceSpMat2D.from_host(SpMat2D(g[f"A0_{i}"], offx, offy))
+        FL.set_brox_matrix(A, cuda32(g[f"psi_{i}"]), float(g["alpha"]))
+        ax = FL.spmv_dia2d(A, cuda32(g[f"x_{i}"]))
+        y0, y1 = FL.apply_brox_preconditioner(A, *(cuda32(g[f"{k}_{i}"]) for k in ("d0", "d1", "od", "x0", "x1")))
+        torch.cuda.synchronize()
+        assert_bitexact(A.data().cpu().numpy(), g[f"A_{i}"], f"A {i}")
+        assert_bitexact(ax.cpu().numpy(), g[f"ax_{i}"], f"ax {i}")
+        assert_bitexact(y0.cpu().numpy(), g[f"y0_{i}"], f"y0 {i}")
+        assert_bitexact(y1.cpu().numpy(), g[f"y1_{i}"], f"y1 {i}")
+        ox4, oy4 = np.delete(offx, 2), np.delete(offy, 2)
+        B = FL.DeviceSpMat2D.from_host(SpMat2D(g[f"R0_{i}"], ox4, oy4))
+        adiag = FL.set_brox_redblack_matrix(B, cuda32(g[f"psi_{i}"]), float(g["alpha"]))
+        torch.cuda.synchronize()
+        assert_bitexact(B.data().cpu().numpy(), g[f"R_{i}"], f"R {i}")
+        assert_bitexact(adiag.cpu().numpy(), g[f"adiag_{i}"], f"adiag {i}")
 
 
 @pytest.mark.parametrize("shape", [(1, 1), (2, 7), (33, 65)])

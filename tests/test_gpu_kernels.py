@@ -45,6 +45,16 @@ def test_stencil2d_golden(cuda, path, pad):
         assert_bitexact(host(out), ref, f"{path} {i}")
 
 
+@pytest.mark.parametrize("pad", [0, 3])
+def test_stencil2d_against_reference_template_golden(cuda, pad):
+    """Stencil2DMVM's device template run as C (clamped taps, accumulation from 0 in tap
+    order), including an asymmetric 6-tap stencil with offsets up to 5: bit-identical."""
+    g = golden("tmpl_stencil.npz")
+    for i in range(int(g["n"])):
+        out = D.stencil2d(g[f"w_{i}"], g[f"offx_{i}"], g[f"offy_{i}"], dev(g[f"x_{i}"], pad))
+        assert_bitexact(host(out), g[f"out_{i}"], f"case {i}")
+
+
 def test_pointwise_ops(cuda):
     rng = np.random.default_rng(1)
     b = rng.standard_normal((37, 45)).astype(np.float32)

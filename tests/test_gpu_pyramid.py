@@ -86,7 +86,7 @@ def test_warp_bitexact(cuda, shape, amp):
 
 def test_warp_against_reference_template_golden(cuda):
     """hs_warp against the reference's WarpImg2D device template run as C: bit-identical."""
-    g = golden("warp_template.npz")
+    g = golden("tmpl_warp.npz")
     for i in range(int(g["n"])):
         out = PY.warp(cuda32(g[f"src_{i}"]), cuda32(g[f"ox_{i}"]), cuda32(g[f"oy_{i}"]))
         torch.cuda.synchronize()

@@ -57,7 +57,7 @@ def test_warp_matches_reference_template_golden():
     """Fractional offsets (integer, -0 and tiny negative ones among them) against the
     reference's WarpImg2D device template run as C (tests/golden/make_template_golden.py):
     both restatements bit-identical, C's left-to-right float/double typing included."""
-    g = golden("warp_template.npz")
+    g = golden("tmpl_warp.npz")
     for i in range(int(g["n"])):
         src, ox, oy = g[f"src_{i}"], g[f"ox_{i}"], g[f"oy_{i}"]
         assert_bitexact(O.c_warp(src, ox, oy), g[f"out_{i}"], f"C, case {i}")
@@ -67,7 +67,7 @@ def test_warp_matches_reference_template_golden():
 def test_matrix_powers_matches_reference_template_golden():
     """HSMatrixPowers' device template (copy into plane 0, one launch per step) run as C
     (tests/golden/make_template_golden.py) against the C restatement: bit-identical."""
-    g = golden("matrix_powers.npz")
+    g = golden("tmpl_matrix_powers.npz")
     for i in range(int(g["n"])):
         V0, V1 = O.c_hs_matrix_powers(g[f"lam_{i}"], g[f"Ix_{i}"], g[f"Iy_{i}"], g[f"r0_{i}"],
                                       g[f"r1_{i}"], int(g[f"steps_{i}"]))
@@ -224,6 +224,32 @@ def test_hs_average_is_self_adjoint():
                                    rtol=0, atol=1e-15)
 
 
+def test_stencil_precond_brox_oracles_match_reference_templates():
+    """Stencil2DMVM, ApplyHSPreconditioner (determinants at float(1e-15)), SetBroxMatrix,
+    SetBroxRedblackMatrix, SpmvDIA2D and ApplyBroxPreconditioner: the reference's device
+    templates run as C (tests/golden/make_template_golden.py) against the restatements."""
+    g = golden("tmpl_stencil.npz")
+    for i in range(int(g["n"])):
+        args = (g[f"w_{i}"], g[f"offx_{i}"], g[f"offy_{i}"], g[f"x_{i}"])
+        assert_bitexact(O.c_stencil2d(*args), g[f"out_{i}"], f"stencil C {i}")
+        assert_bitexact(O.stencil2d(*args), g[f"out_{i}"], f"stencil NumPy {i}")
+    g = golden("tmpl_precond.npz")
+    for i in range(int(g["n"])):
+        y0, y1 = O.c_apply_hs_precond(g[f"s2_{i}"], *(g[f"{k}_{i}"] for k in ("d0", "d1", "od", "x0", "x1")))
+        assert_bitexact(y0, g[f"y0_{i}"], f"precond {i}")
+        assert_bitexact(y1, g[f"y1_{i}"], f"precond {i}")
+    g = golden("tmpl_brox.npz")
+    for i in range(int(g["n"])):
+        assert_bitexact(O.c_set_brox_matrix(g[f"psi_{i}"], g["alpha"], g[f"A0_{i}"]), g[f"A_{i}"])
+        R, adiag = O.c_set_brox_matrix(g[f"psi_{i}"], g["alpha"], g[f"R0_{i}"], redblack=True)
+        assert_bitexact(R, g[f"R_{i}"])
+        assert_bitexact(adiag, g[f"adiag_{i}"])
+        assert_bitexact(O.c_spmv_dia2d(g[f"A_{i}"], O.BROX_OFFX, O.BROX_OFFY, g[f"x_{i}"]), g[f"ax_{i}"])
+        y0, y1 = O.c_apply_brox_precond(g[f"A_{i}"][2], *(g[f"{k}_{i}"] for k in ("d0", "d1", "od", "x0", "x1")))
+        assert_bitexact(y0, g[f"y0_{i}"])
+        assert_bitexact(y1, g[f"y1_{i}"])
+
+
 def test_precond_oracle_matches_reference_golden():
     """ApplyHSPreconditioner restatement vs hlib.applyHSPreconditioner (golden fixtures):
     bit-identical where both determinant guards agree (all of the fixtures)."""
@@ -274,7 +300,7 @@ def test_lk_oracle_matches_reference_template_golden():
     """The LKLeastSquares restatement against the reference's own device template
     (LKLeastSquares.cpp:39-91), instantiated as C by tests/golden/make_template_golden.py:
     bit-identical, including the border rule and det == 0 windows."""
-    g = golden("lk.npz")
+    g = golden("tmpl_lk.npz")
     for i in range(int(g["n"])):
         du, dv = O.c_lk_least_squares(g[f"err_{i}"], g[f"Ix_{i}"], g[f"Iy_{i}"], int(g[f"rad_{i}"]))
         assert_bitexact(du, g[f"du_{i}"], f"case {i}")
