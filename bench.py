@@ -169,7 +169,7 @@ def cpu_leg_timings(I0, I1, alpha, args):
     O.lib()
     cores = O.c_num_threads()
     sweeps = args.cpu_sample_sweeps
-    value, _ = c1_sample_rate(O, I0, I1, alpha, sweeps, args.steps)
+    value, _ = c1_sample_rate(O, I0, I1, alpha, sweeps, args.steps, warm=max(args.warmup, 1))
     H, W = I0.shape
     out = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
            "sample": f"{W}x{H}, {sweeps} sweeps per step x {args.steps} warm steps (bounded "
@@ -929,17 +929,6 @@ def main():
     from hindemith_b200 import autotune
     from hindemith_b200.replicas import job_rate, max_over_ranks, rank_seed
 
-    if not torch.cuda.is_available():
-        raise SystemExit("bench.py: no CUDA device (libhsflow has no CPU path)")
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    warmup = max(args.warmup, 3)
-
     spec = synthetic.plain_1080p()
     spec.seed = rank_seed(spec.seed, rank)
     workload = "hs_plain_1920x1080_500sweeps"
@@ -952,8 +941,21 @@ def main():
     I0h, I1h, _, _ = synthetic.generate(spec)
     H, W, iters, alpha = spec.H, spec.W, spec.iters, spec.alpha
     cpu_leg = rank == 0 and world == 1 and not args.no_cpu_baseline
-    # the CPU baseline runs first, on an idle host, with the same warm loop as --impl reference
+    # The CPU baseline runs first, before this process touches CUDA (the driver's threads
+    # take host cycles once a context exists: about 20 % of the 16-core rate was measured
+    # lost), with the same warm loop as --impl reference.
     cpu_times = cpu_leg_timings(I0h, I1h, alpha, args) if cpu_leg else None
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device (libhsflow has no CPU path)")
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    warmup = max(args.warmup, 3)
     checks = {}
     I0 = D.as_plane(torch.from_numpy(I0h).cuda())
     I1 = D.as_plane(torch.from_numpy(I1h).cuda())
