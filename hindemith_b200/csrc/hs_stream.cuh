@@ -16,7 +16,7 @@
 //     both columns' operation in one instruction, each rounded as its scalar form, so the
 //     results are those of the scalar operation sequence bit for bit (the exact form's
 //     products stay scalar multiplies, which are never fused into the adds).
-// A strip loads `halo` extra columns each side (T rounded up to a multiple of 4) and
+// A strip loads `halo` extra columns each side (T rounded up to an even count) and
 // outputs the middle 64 - 2*halo; a segment starts T rows early; both are the temporal
 // blocking halo.  Warps never synchronise with each other; within a warp, a barrier after
 // each row's cp.async wait publishes the lanes' copies to the lanes that read them.

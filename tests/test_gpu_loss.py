@@ -26,7 +26,7 @@ def test_mean_epe_batch_matches_float64(cuda, shapes):
     ref = sum(torch.sqrt((u - ut) ** 2 + (v - vt) ** 2 + 1e-12).mean()
               for (u, v), (ut, vt) in zip(f64, t64)) / len(f64)
     (2.5 * ref).backward()
-    assert abs(float(loss) - float(ref)) <= 1e-6 * abs(float(ref))
+    assert abs(float(loss.detach()) - float(ref.detach())) <= 1e-6 * abs(float(ref.detach()))
     for (u, v), (ur, vr) in zip(flows, f64):
         for g, r in ((u.grad, ur.grad), (v.grad, vr.grad)):
             err = np.abs(g.cpu().numpy() - r.numpy()).max() / np.abs(r.numpy()).max()
