@@ -129,10 +129,10 @@ struct Win<false> {
 // and advances the window.  EDGE: the row may be row 0 (top clamp) or past the bottom
 // (replaced by row H-1, the bottom clamp).  The fast form has no product feeding an add
 // (mul2's restriction).
+// The fast form from the row's horizontal neighbour sums hn = left + right.
 template <bool EDGE>
-__device__ __forceinline__ float2 win_step(Win<true> &w, float2 l, float2 c, float2 r, int n, int H,
-                                           float2 we, float2 wc) {
-    const float2 hn = add2(l, r);
+__device__ __forceinline__ float2 win_step_h(Win<true> &w, float2 hn, float2 c, int n, int H,
+                                             float2 we, float2 wc) {
     float2 yn = fma2(we, c, mul2(wc, hn));
     if (EDGE && n >= H) yn = w.Y1;  // the row below H-1 is row H-1
     const float2 out = add2(w.Z, yn);
@@ -255,13 +255,25 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
             const float2 c = cu[q];
             const float fromL = __shfl_up_sync(kFull, c.y, 1);
             const float fromR = __shfl_down_sync(kFull, c.x, 1);
-            float2 l = f2(fromL, c.x), r = f2(c.y, fromR);
-            if constexpr (XEDGE) {
-                l.x = it.a_first ? c.x : l.x;
-                r.x = it.a_last ? c.x : r.x;
-                r.y = it.b_last ? c.y : r.y;
+            if constexpr (FAST) {
+                // left + right of both columns as scalar adds straight into their pair
+                float L = fromL, R0 = c.y, R1 = fromR;
+                if constexpr (XEDGE) {
+                    L = it.a_first ? c.x : L;
+                    R0 = it.a_last ? c.x : R0;
+                    R1 = it.b_last ? c.y : R1;
+                }
+                const float2 h = f2(__fadd_rn(L, R0), __fadd_rn(c.x, R1));
+                ub[q] = win_step_h<EDGE>(w[s][q], h, c, n, p.H, we2, wc2);
+            } else {
+                float2 l = f2(fromL, c.x), r = f2(c.y, fromR);
+                if constexpr (XEDGE) {
+                    l.x = it.a_first ? c.x : l.x;
+                    r.x = it.a_last ? c.x : r.x;
+                    r.y = it.b_last ? c.y : r.y;
+                }
+                ub[q] = win_step<EDGE>(w[s][q], l, c, r, n, p.H, we2, wc2);
             }
-            ub[q] = win_step<EDGE>(w[s][q], l, c, r, n, p.H, we2, wc2);
         }
         // pointwise update of row n-1 with its coefficients
         int rs = cslot - (s + 1);

@@ -12,12 +12,13 @@
 //   - the per-step bookkeeping (copies, ring indices, stores) is spread over twice the
 //     cells, and the temporal halo (T rounded up to 4 columns each side) is a smaller share
 //     of the strip (120 or 112 output columns of 128).
-// The arithmetic runs on column pairs with the sm_100 packed FP32 instructions (one
-// instruction, two IEEE operations rounded as their scalar forms): the pairs are columns
-// (0, 2) and (1, 3), so each pair's horizontal neighbours are the other pair plus one
-// shuffled value, and the coefficient ring holds -1/den so the update is three packed
-// FMAs and one packed multiply per pair; results equal the scalar 2-column kernel's bit for
-// bit.  Only the fast form (FMA, reciprocal of the denominator) exists in this layout; the
+// The arithmetic runs on column pairs (0, 1) and (2, 3) with the sm_100 packed FP32
+// instructions (one instruction, two IEEE operations rounded as their scalar forms).  The
+// pairs are the halves of the lane's 16-byte chunk as loaded, the coefficient ring holds each
+// coefficient's 4 columns as loaded (Ix, Iy, It and -1/den), and the horizontal neighbour
+// sums left + right are formed as scalar adds straight into their pair: no value is moved
+// to repack a pair.  The update is then three packed FMAs and one packed multiply per pair;
+// results equal the scalar 2-column kernel's bit for bit.  Only the fast form (FMA, reciprocal of the denominator) exists in this layout; the
 // exact form keeps the 2-column layout, whose tap-ordered windows need 5 registers per column.
 #pragma once
 
@@ -35,14 +36,14 @@ struct GeoW {
     static constexpr int strip = kWideCols - 2 * halo;         // output columns per strip
     static constexpr int coef_slots = T + 1;                   // rows k-T .. k
     static constexpr int raw_floats = kWideRawSlots * kRawPlanes * kWideCols;
-    static constexpr int coef_floats = coef_slots * 4 * 32 * 4;  // [slot][4][lane] float4
+    static constexpr int coef_floats = coef_slots * 4 * 32 * 4;  // [slot][coef][lane] float4
     static constexpr int warp_floats = raw_floats + coef_floats;
     static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
 };
 
 struct ItemW {
     float *raw;     // [kWideRawSlots][kRawPlanes][128]
-    float4 *coef;   // [T+1][4][32]: per pair (0,2) then (1,3): (Ix, Iy) then (It, -1/den)
+    float4 *coef;   // [T+1][4][32]: Ix, Iy, It, -1/den of the lane's 4 columns
     int lane;
     int lcol;       // this lane's chunk, clamped to an in-bounds chunk of the row
     int xa;         // first of the lane's 4 columns
@@ -82,25 +83,26 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
     issue_row_w(it, rslot == 0 ? kWideRawSlots - 1 : rslot - 1, min(k + kWidePrefetch, it.y_end - 1 + T), p);
     cp_async_wait<kWidePrefetch>();
 
-    // stage 0: unpack row k; pack its coefficients per column pair with -1/den
+    // stage 0: unpack row k; keep its coefficients as loaded, with -1/den
     const float *raw = it.raw + rslot * (kRawPlanes * kWideCols) + 4 * it.lane;
     const float4 u4 = lds4(raw), v4 = lds4(raw + kWideCols);
     {
         const float4 ix = lds4(raw + 2 * kWideCols), iy = lds4(raw + 3 * kWideCols);
         const float4 t4 = lds4(raw + 4 * kWideCols);
-        const float n0 = -rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
-        const float n1 = -rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
-        const float n2 = -rcp_approx(fmaf(iy.z, iy.z, fmaf(ix.z, ix.z, it.alpha2)));
-        const float n3 = -rcp_approx(fmaf(iy.w, iy.w, fmaf(ix.w, ix.w, it.alpha2)));
+        float4 nw;
+        nw.x = -rcp_approx(fmaf(iy.x, iy.x, fmaf(ix.x, ix.x, it.alpha2)));
+        nw.y = -rcp_approx(fmaf(iy.y, iy.y, fmaf(ix.y, ix.y, it.alpha2)));
+        nw.z = -rcp_approx(fmaf(iy.z, iy.z, fmaf(ix.z, ix.z, it.alpha2)));
+        nw.w = -rcp_approx(fmaf(iy.w, iy.w, fmaf(ix.w, ix.w, it.alpha2)));
         float4 *cs = it.coef + cslot * 128 + it.lane;
-        cs[0] = make_float4(ix.x, ix.z, iy.x, iy.z);
-        cs[32] = make_float4(t4.x, t4.z, n0, n2);
-        cs[64] = make_float4(ix.y, ix.w, iy.y, iy.w);
-        cs[96] = make_float4(t4.y, t4.w, n1, n3);
+        cs[0] = ix;
+        cs[32] = iy;
+        cs[64] = t4;
+        cs[96] = nw;
     }
-    // [plane][pair]: pair 0 holds columns (0, 2), pair 1 columns (1, 3)
-    float2 cu[2][2] = {{make_float2(u4.x, u4.z), make_float2(u4.y, u4.w)},
-                       {make_float2(v4.x, v4.z), make_float2(v4.y, v4.w)}};
+    // [plane][pair]: pair 0 holds columns (0, 1), pair 1 columns (2, 3)
+    float2 cu[2][2] = {{make_float2(u4.x, u4.y), make_float2(u4.z, u4.w)},
+                       {make_float2(v4.x, v4.y), make_float2(v4.z, v4.w)}};
     const float2 we2 = make_float2(p.we, p.we), wc2 = make_float2(p.wc, p.wc);
 
 #pragma unroll
@@ -110,32 +112,36 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
         float2 ub[2][2];
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
-            const float2 E = cu[q][0], O = cu[q][1];  // (c0, c2), (c1, c3)
+            const float2 E = cu[q][0], O = cu[q][1];  // (c0, c1), (c2, c3)
             const float lsh = __shfl_up_sync(kFull, O.y, 1);    // column -1: lane-1's c3
             const float rsh = __shfl_down_sync(kFull, E.x, 1);  // column 4: lane+1's c0
-            float2 lE = make_float2(lsh, O.x), rE = O;          // neighbours of (c0, c2)
-            float2 rO = make_float2(E.y, rsh);                  // right of (c1, c3); left is E
+            // left and right neighbours: the column itself at an image side
+            float L0 = lsh, R0 = E.y, R1 = O.x, R2 = O.y, R3 = rsh;
             if constexpr (XE == 1) {
-                lE.x = it.first ? E.x : lE.x;
-                rE.x = (it.last & 1u) ? E.x : rE.x;
-                rO.x = (it.last & 2u) ? O.x : rO.x;
-                rE.y = (it.last & 4u) ? E.y : rE.y;
-                rO.y = (it.last & 8u) ? O.y : rO.y;
+                L0 = it.first ? E.x : L0;
+                R0 = (it.last & 1u) ? E.x : R0;
+                R1 = (it.last & 2u) ? E.y : R1;
+                R2 = (it.last & 4u) ? O.x : R2;
+                R3 = (it.last & 8u) ? O.y : R3;
             } else if constexpr (XE == 2) {
-                lE.x = it.first ? E.x : lE.x;
-                rO.y = (it.last & 8u) ? O.y : rO.y;
+                L0 = it.first ? E.x : L0;
+                R3 = (it.last & 8u) ? O.y : R3;
             }
-            ub[q][0] = win_step<EDGE>(w[s][q][0], lE, E, rE, n, p.H, we2, wc2);
-            ub[q][1] = win_step<EDGE>(w[s][q][1], E, O, rO, n, p.H, we2, wc2);
+            const float2 hE = make_float2(__fadd_rn(L0, R0), __fadd_rn(E.x, R1));
+            const float2 hO = make_float2(__fadd_rn(E.y, R2), __fadd_rn(O.x, R3));
+            ub[q][0] = win_step_h<EDGE>(w[s][q][0], hE, E, n, p.H, we2, wc2);
+            ub[q][1] = win_step_h<EDGE>(w[s][q][1], hO, O, n, p.H, we2, wc2);
         }
         int rs = cslot - (s + 1);
         if (rs < 0) rs += GeoW<T>::coef_slots;
         const float4 *cr = it.coef + rs * 128 + it.lane;
+        const float4 cX = cr[0], cY = cr[32], cT = cr[64], cN = cr[96];
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
-            const float4 A = cr[64 * j], B = cr[64 * j + 32];
-            const float2 cx = make_float2(A.x, A.y), cy = make_float2(A.z, A.w);
-            const float2 ct = make_float2(B.x, B.y), nw = make_float2(B.z, B.w);
+            const float2 cx = j ? make_float2(cX.z, cX.w) : make_float2(cX.x, cX.y);
+            const float2 cy = j ? make_float2(cY.z, cY.w) : make_float2(cY.x, cY.y);
+            const float2 ct = j ? make_float2(cT.z, cT.w) : make_float2(cT.x, cT.y);
+            const float2 nw = j ? make_float2(cN.z, cN.w) : make_float2(cN.x, cN.y);
             const float2 ubar = ub[0][j], vbar = ub[1][j];
             // -t = (Ix ubar + Iy vbar + It) * (-1/den); u = ubar + Ix (-t) = ubar - Ix t
             const float2 nt = mul2(fma2(cx, ubar, fma2(cy, vbar, ct)), nw);
@@ -146,8 +152,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
             const int rr = k - s - 1;
             if (rr >= it.y_start && rr < it.y_end) {
                 const size_t off = (size_t)rr * p.ld + it.xa;
-                const float du[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
-                const float dv[4] = {cu[1][0].x, cu[1][1].x, cu[1][0].y, cu[1][1].y};
+                const float du[4] = {cu[0][0].x, cu[0][0].y, cu[0][1].x, cu[0][1].y};
+                const float dv[4] = {cu[1][0].x, cu[1][0].y, cu[1][1].x, cu[1][1].y};
                 if (it.st == 15u) {
                     *reinterpret_cast<float4 *>(p.dump_u[s] + off) = make_float4(du[0], du[1], du[2], du[3]);
                     *reinterpret_cast<float4 *>(p.dump_v[s] + off) = make_float4(dv[0], dv[1], dv[2], dv[3]);
@@ -167,8 +173,8 @@ __device__ __forceinline__ void stream_step_w(const SweepParams &p, const ItemW 
     const int r = k - T;
     if (r >= it.y_start && r < it.y_end) {
         const size_t off = (size_t)r * p.ld + it.xa;
-        const float uo[4] = {cu[0][0].x, cu[0][1].x, cu[0][0].y, cu[0][1].y};
-        const float vo[4] = {cu[1][0].x, cu[1][1].x, cu[1][0].y, cu[1][1].y};
+        const float uo[4] = {cu[0][0].x, cu[0][0].y, cu[0][1].x, cu[0][1].y};
+        const float vo[4] = {cu[1][0].x, cu[1][0].y, cu[1][1].x, cu[1][1].y};
         if (it.st == 15u) {
             *reinterpret_cast<float4 *>(p.u_out + off) = make_float4(uo[0], uo[1], uo[2], uo[3]);
             *reinterpret_cast<float4 *>(p.v_out + off) = make_float4(vo[0], vo[1], vo[2], vo[3]);
