@@ -96,7 +96,8 @@ def test_sweeps_exact_golden(cuda, path, T):
 
 
 @pytest.mark.parametrize("shape", [(1, 1), (1, 2), (1, 67), (67, 1), (2, 2), (3, 5), (5, 3),
-                                   (7, 130), (130, 7), (64, 64), (65, 127)])
+                                   (7, 130), (130, 7), (64, 64), (65, 127), (50, 4), (33, 500),
+                                   (97, 256)])
 @pytest.mark.parametrize("T", ALL_T)
 def test_sweeps_exact_edge_shapes(cuda, shape, T):
     H, W = shape
