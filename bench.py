@@ -322,6 +322,14 @@ def cpu_baselines_other():
     return out
 
 
+def headline_config(workload, H, W, iters, alpha, world):
+    """The headline workload's config, one dict for both arms (GPU and host cores)."""
+    return {"workload": workload, "H": H, "W": W, "iters": iters, "alpha": alpha,
+            "pairs_per_rank": 1, "parallelism": f"replicas x{world}",
+            "l2": "GPU arm: flushed between steps (256 MiB write); the 41 MB working set of "
+                  "one pair is L2-resident within a step"}
+
+
 def run_reference(args, rank, world):
     """--impl reference: the host-core restatement of the reference's kernels."""
     from hindemith_b200 import synthetic
@@ -342,11 +350,10 @@ def run_reference(args, rank, world):
             "warmup": args.warmup, "ms_per_step": tot / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "hs_plain_1920x1080_500sweeps", "H": spec.H, "W": spec.W,
-                       "iters": spec.iters, "alpha": spec.alpha, "pairs_per_rank": 1,
-                       "parallelism": f"replicas x{world} (rank 0 runs the host cores)",
-                       "l2": "host run: no GPU L2"},
+            "config": headline_config("hs_plain_1920x1080_500sweeps", spec.H, spec.W, spec.iters,
+                                      spec.alpha, world),
             "sample_sweeps_per_step": sweeps,
+            "host_run": "rank 0 runs the host cores; no GPU L2 is involved",
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -1102,10 +1109,7 @@ def main():
         "warmup": warmup, "ms_per_step": t_step / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded blurred noise + sinusoidal flow; see hindemith_b200/synthetic.py)",
-        "config": {"workload": workload, "H": H, "W": W, "iters": iters, "alpha": alpha,
-                   "pairs_per_rank": 1, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (256 MiB write); the 41 MB working set of one "
-                         "pair is L2-resident within a step"},
+        "config": headline_config(workload, H, W, iters, alpha, world),
         "tuning": {"sweeps_per_pass": T, "rows_per_segment": seg,
                    "columns_per_lane": 4 if wide else 2, "fast_math": not args.exact,
                    "autotuned": args.sweeps_per_pass == 0},
