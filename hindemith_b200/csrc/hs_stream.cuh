@@ -40,7 +40,13 @@ constexpr int kWarpCols = 64;                 // columns per strip (2 per lane)
 constexpr int kPrefetch = 3;                  // rows in flight per warp
 constexpr int kRawSlots = kPrefetch + 1;      // raw-row ring depth (a power of two)
 constexpr int kRawPlanes = 5;                 // u, v, Ix, Iy, It as copied from HBM
-constexpr int kWarpsPerBlock = 4;             // independent warps per CTA
+constexpr int kWarpsPerBlock = 4;             // independent warps per CTA (persistent batch)
+// Warps per CTA of the per-pass launches (the plain sweep and the training table and adjoint
+// passes).  Each warp is an independent work item, so a one-warp CTA frees its slot the moment
+// its item ends: another item, or the next pass's first items under programmatic dependent
+// launch, start there at once instead of waiting for the CTA's slowest warp.  The resident
+// warps per SM (each kernel's register budget) stay those of 4-warp CTAs.
+constexpr int kPassWarps = 1;
 constexpr unsigned kFull = 0xffffffffu;
 
 template <int T>

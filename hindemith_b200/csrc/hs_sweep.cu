@@ -7,12 +7,12 @@
 
 namespace hs {
 
-// Resident CTAs per SM the register budget is sized for (shared memory allows it too).
-// (Measured: capping registers for more CTAs costs more ILP than it gains.)
-constexpr int min_blocks(int T) { return T <= 4 ? 4 : (T <= 6 ? 3 : 2); }
+// Resident warps per SM the register budget is sized for (shared memory allows it too).
+// (Measured: capping registers for more warps costs more ILP than it gains.)
+constexpr int res_warps(int T) { return T <= 4 ? 16 : (T <= 6 ? 12 : 8); }
 
 template <int T, bool FAST>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks(T))
+__global__ void __launch_bounds__(kPassWarps * 32, res_warps(T) / kPassWarps)
     hs_stream_kernel(const SweepParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks(T))
     griddep_launch_dependents();
     griddep_wait();
 
-    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    const int item = blockIdx.x * kPassWarps + warp;
     if (item >= p.nitems) return;  // warp-uniform
     Item it;
     init_item<T>(it, p, item % p.nstrips, item / p.nstrips, lane, wbase);
@@ -30,10 +30,10 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks(T))
 }
 
 // The fast form in the wide layout (hs_stream4.cuh).
-constexpr int min_blocks_w(int T) { return T <= 4 ? 3 : 2; }
+constexpr int res_warps_w(int T) { return T <= 4 ? 12 : 8; }
 
 template <int T>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks_w(T))
+__global__ void __launch_bounds__(kPassWarps * 32, res_warps_w(T) / kPassWarps)
     hs_stream_w_kernel(const SweepParams p) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, min_blocks_w(T))
     griddep_launch_dependents();
     griddep_wait();
 
-    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    const int item = blockIdx.x * kPassWarps + warp;
     if (item >= p.nitems) return;  // warp-uniform
     ItemW it;
     init_item_w<T>(it, p, item % p.nstrips, item / p.nstrips, lane, wbase);
@@ -63,8 +63,8 @@ static hs_status launch_kernel(KernelFn fn, int smem, bool *attr_set, const Swee
         attr_set[dev] = true;
     }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((pp.nitems + kWarpsPerBlock - 1) / kWarpsPerBlock));
-    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.gridDim = dim3((unsigned)((pp.nitems + kPassWarps - 1) / kPassWarps));
+    cfg.blockDim = dim3(kPassWarps * 32);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
@@ -79,7 +79,8 @@ static hs_status launch_kernel(KernelFn fn, int smem, bool *attr_set, const Swee
 template <int T>
 static hs_status launch_one_w(const SweepParams &pp, cudaStream_t stream) {
     static bool attr_set[64] = {};
-    return launch_kernel(hs_stream_w_kernel<T>, GeoW<T>::smem_bytes, attr_set, pp, stream);
+    return launch_kernel(hs_stream_w_kernel<T>, kPassWarps * GeoW<T>::warp_floats * (int)sizeof(float),
+                         attr_set, pp, stream);
 }
 
 int strip_cols_wide(int T) {
@@ -118,13 +119,13 @@ static hs_status launch_one(const SweepParams &pp, cudaStream_t stream) {
     cudaGetDevice(&dev);
     if (dev < 64 && !attr_set[dev]) {
         HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           G::smem_bytes));
+                                           kPassWarps * G::warp_floats * (int)sizeof(float)));
         attr_set[dev] = true;
     }
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((pp.nitems + kWarpsPerBlock - 1) / kWarpsPerBlock));
-    cfg.blockDim = dim3(kWarpsPerBlock * 32);
-    cfg.dynamicSmemBytes = G::smem_bytes;
+    cfg.gridDim = dim3((unsigned)((pp.nitems + kPassWarps - 1) / kPassWarps));
+    cfg.blockDim = dim3(kPassWarps * 32);
+    cfg.dynamicSmemBytes = kPassWarps * G::warp_floats * (int)sizeof(float);
     cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -251,7 +252,7 @@ hs_status run_passes_dev(const float *Ix, const float *Iy, const float *It, int 
         const int sc = wide ? strip_cols_wide(t) : strip_cols_for(t);
         pp.nstrips = (W + sc - 1) / sc;
         pp.seg_rows = rc.seg_rows > 0 ? std::min(rc.seg_rows, H)
-                                      : seg_rows_for(H, pp.nstrips, t, wide ? kWarpsPerBlock * min_blocks_w(t) : 16);
+                                      : seg_rows_for(H, pp.nstrips, t, wide ? res_warps_w(t) : 16);
         const int nseg = (H + pp.seg_rows - 1) / pp.seg_rows;
         pp.nitems = pp.nstrips * nseg;
         hs_status st = wide ? launch_pass_w(t, pp, stream) : launch_pass(t, rc.fast, pp, stream);

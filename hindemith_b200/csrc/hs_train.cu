@@ -34,6 +34,12 @@ constexpr int kMaxTB = 5;
 constexpr int kAdjMaxDepth = 4;     // deepest adjoint pass the backward plans
 constexpr int kAdjItemsPerSmMax = 16;  // adjoint work items (warps) per SM and launch, at most
 constexpr int kMinStripCols = 52;   // narrowest adjoint strip (depth <= 5): 64 less 6 each side
+// Warps per CTA of the backward's launches.  Its recompute (dump) passes and adjoint passes
+// run on two streams at once; with 4-warp CTAs each SM holds blocks of one kind, while one-warp
+// CTAs interleave the two kinds warp by warp on every SM (measured on B200, 16 x 512^2, 200
+// sweeps: forward + backward 9.1 ms against 10.2 ms with one-warp dump passes).  The forward's
+// passes run alone and use one-warp CTAs (kPassWarps).
+constexpr int kBackwardWarps = 4;
 
 // ------------------------------------------------------------------ table-driven pass
 
@@ -54,8 +60,8 @@ __device__ __forceinline__ int find_pair(const int *prefix, int n, int item) {
     return lo;
 }
 
-template <int T, bool FAST>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3 : 2)))
+template <int T, bool FAST, int WP>
+__global__ void __launch_bounds__(WP * 32, (T <= 4 ? 16 : (T <= 6 ? 12 : 8)) / WP)
     hs_table_pass_kernel(const __grid_constant__ PassTable tab) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -63,7 +69,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
     float *wbase = reinterpret_cast<float *>(smem4) + warp * Geo<T>::warp_floats;
     griddep_launch_dependents();
     griddep_wait();
-    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    const int item = blockIdx.x * WP + warp;
     if (item >= tab.item_prefix[tab.npairs]) return;
     const int pi = find_pair(tab.item_prefix, tab.npairs, item);
     const SweepParams &p = tab.pair[pi];
@@ -74,21 +80,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 4 : (T <= 6 ? 3
     else run_item<T, FAST, false>(p, it);
 }
 
-template <int T, bool FAST>
-static hs_status launch_table(const PassTable &tab, cudaStream_t s) {
-    auto fn = hs_table_pass_kernel<T, FAST>;
+template <int T, bool FAST, int WP>
+static hs_status launch_table_wp(const PassTable &tab, cudaStream_t s) {
+    auto fn = hs_table_pass_kernel<T, FAST, WP>;
     static bool attr[64] = {};
     int dev = 0;
     HS_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, Geo<T>::smem_bytes));
+        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           WP * Geo<T>::warp_floats * (int)sizeof(float)));
         attr[dev] = true;
     }
     const int items = tab.item_prefix[tab.npairs];
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
-    cfg.blockDim = dim3(kWarpsPerBlock * 32);
-    cfg.dynamicSmemBytes = Geo<T>::smem_bytes;
+    cfg.gridDim = dim3((unsigned)((items + WP - 1) / WP));
+    cfg.blockDim = dim3(WP * 32);
+    cfg.dynamicSmemBytes = WP * Geo<T>::warp_floats * (int)sizeof(float);
     cfg.stream = s;
     cudaLaunchAttribute a[1];
     a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -100,8 +107,8 @@ static hs_status launch_table(const PassTable &tab, cudaStream_t s) {
 }
 
 // The same pass in the 4-columns-per-lane layout (fast form only).
-template <int T>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 3 : 2))
+template <int T, int WP>
+__global__ void __launch_bounds__(WP * 32, (T <= 4 ? 12 : 8) / WP)
     hs_table_pass_w_kernel(const __grid_constant__ PassTable tab) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -109,7 +116,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 3 : 2))
     float *wbase = reinterpret_cast<float *>(smem4) + warp * GeoW<T>::warp_floats;
     griddep_launch_dependents();
     griddep_wait();
-    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    const int item = blockIdx.x * WP + warp;
     if (item >= tab.item_prefix[tab.npairs]) return;
     const int pi = find_pair(tab.item_prefix, tab.npairs, item);
     const SweepParams &p = tab.pair[pi];
@@ -120,21 +127,22 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, (T <= 4 ? 3 : 2))
     else run_item_w<T, false>(p, it);
 }
 
-template <int T>
-static hs_status launch_table_w(const PassTable &tab, cudaStream_t s) {
-    auto fn = hs_table_pass_w_kernel<T>;
+template <int T, int WP>
+static hs_status launch_table_w_wp(const PassTable &tab, cudaStream_t s) {
+    auto fn = hs_table_pass_w_kernel<T, WP>;
     static bool attr[64] = {};
     int dev = 0;
     HS_CUDA_CHECK(cudaGetDevice(&dev));
     if (dev < 64 && !attr[dev]) {
-        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, GeoW<T>::smem_bytes));
+        HS_CUDA_CHECK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           WP * GeoW<T>::warp_floats * (int)sizeof(float)));
         attr[dev] = true;
     }
     const int items = tab.item_prefix[tab.npairs];
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
-    cfg.blockDim = dim3(kWarpsPerBlock * 32);
-    cfg.dynamicSmemBytes = GeoW<T>::smem_bytes;
+    cfg.gridDim = dim3((unsigned)((items + WP - 1) / WP));
+    cfg.blockDim = dim3(WP * 32);
+    cfg.dynamicSmemBytes = WP * GeoW<T>::warp_floats * (int)sizeof(float);
     cfg.stream = s;
     cudaLaunchAttribute a[1];
     a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -143,6 +151,22 @@ static hs_status launch_table_w(const PassTable &tab, cudaStream_t s) {
     cfg.numAttrs = 1;
     HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, fn, tab));
     return HS_OK;
+}
+
+// The forward's passes in one-warp CTAs, the backward's recompute passes (depth <= 5, every
+// pair of a table dumps or none does) in kBackwardWarps.
+constexpr int kMaxDumpDepth = 5;
+template <int T, bool FAST>
+static hs_status launch_table(const PassTable &tab, cudaStream_t s) {
+    if (!tab.pair[0].dump) return launch_table_wp<T, FAST, kPassWarps>(tab, s);
+    if constexpr (T <= kMaxDumpDepth) return launch_table_wp<T, FAST, kBackwardWarps>(tab, s);
+    else HS_FAIL(HS_ERR_INVALID_ARG, "recompute pass depth %d above %d", T, kMaxDumpDepth);
+}
+template <int T>
+static hs_status launch_table_w(const PassTable &tab, cudaStream_t s) {
+    if (!tab.pair[0].dump) return launch_table_w_wp<T, kPassWarps>(tab, s);
+    if constexpr (T <= kMaxDumpDepth) return launch_table_w_wp<T, kBackwardWarps>(tab, s);
+    else HS_FAIL(HS_ERR_INVALID_ARG, "recompute pass depth %d above %d", T, kMaxDumpDepth);
 }
 
 static hs_status launch_table_any(int T, bool fast, const PassTable &tab, cudaStream_t s) {
@@ -192,7 +216,7 @@ struct AdjGeo {
     static constexpr int raw_floats = Geo<TB>::raw_floats;
     static constexpr int ring_floats = coef_slots * 2 * 2 * 32 * 4;  // [slot][4][lane] float4 pairs
     static constexpr int warp_floats = raw_floats + ring_floats;
-    static constexpr int smem_bytes = kWarpsPerBlock * warp_floats * (int)sizeof(float);
+    static constexpr int smem_bytes = kBackwardWarps * warp_floats * (int)sizeof(float);
 };
 
 // M of one sweep at one column: lambda (lu, lv) -> z, adding this sweep's gradient terms to
@@ -392,11 +416,11 @@ __device__ __forceinline__ void adj_item(const AdjPair &P, const SweepParams &lp
     if (it.lane == 0) P.a2part[local] += d;
 }
 
-// resident CTAs per SM the register budget is sized for: depth <= 3 fits 4 (16 warps/SM)
-constexpr int adj_min_blocks(int TB) { return TB <= 3 ? 4 : 3; }
+// resident warps per SM the register budget is sized for: depth <= 3 fits 16
+constexpr int adj_res_warps(int TB) { return TB <= 3 ? 16 : 12; }
 
 template <int TB>
-__global__ void __launch_bounds__(kWarpsPerBlock * 32, adj_min_blocks(TB))
+__global__ void __launch_bounds__(kBackwardWarps * 32, adj_res_warps(TB) / kBackwardWarps)
     hs_adjoint_pass_kernel(const __grid_constant__ AdjTable tab) {
     extern __shared__ float4 smem4[];
     const int lane = threadIdx.x & 31;
@@ -404,7 +428,7 @@ __global__ void __launch_bounds__(kWarpsPerBlock * 32, adj_min_blocks(TB))
     float *wbase = reinterpret_cast<float *>(smem4) + warp * AdjGeo<TB>::warp_floats;
     griddep_launch_dependents();
     griddep_wait();
-    const int item = blockIdx.x * kWarpsPerBlock + warp;
+    const int item = blockIdx.x * kBackwardWarps + warp;
     if (item >= tab.item_prefix[tab.npairs]) return;
     const int pi = find_pair(tab.item_prefix, tab.npairs, item);
     const AdjPair &P = tab.pair[pi];
@@ -444,8 +468,8 @@ static hs_status launch_adj(const AdjTable &tab, cudaStream_t s) {
     }
     const int items = tab.item_prefix[tab.npairs];
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)((items + kWarpsPerBlock - 1) / kWarpsPerBlock));
-    cfg.blockDim = dim3(kWarpsPerBlock * 32);
+    cfg.gridDim = dim3((unsigned)((items + kBackwardWarps - 1) / kBackwardWarps));
+    cfg.blockDim = dim3(kBackwardWarps * 32);
     cfg.dynamicSmemBytes = AdjGeo<TB>::smem_bytes;
     cfg.stream = s;
     cudaLaunchAttribute a[1];
@@ -659,7 +683,7 @@ static void set_segments(PassTable &tab, int T) {
             tab.pair[i].nstrips = (tab.pair[i].W + strip_cols_wide(T) - 1) / strip_cols_wide(T);
     long rows = 0;
     for (int i = 0; i < tab.npairs; ++i) rows += (long)tab.pair[i].nstrips * tab.pair[i].H;
-    const long target = (long)sm_count() * (tab.wide ? kWarpsPerBlock * (T <= 4 ? 3 : 2) : 16);
+    const long target = (long)sm_count() * (tab.wide ? (T <= 4 ? 12 : 8) : 16);
     int L = (int)std::max(1L, (rows + target - 1) / target);
     L = std::max(L, 2 * T);
     tab.item_prefix[0] = 0;
@@ -776,7 +800,7 @@ static hs_status train_backward(const hs_train_pair *pairs, const PairBufs *bufs
         const int nsw = std::min(ckpt_every, iters - b * ckpt_every);
         const int sb = b & 1;
         for (int done = 0; done < nsw - 1;) {
-            const int t = std::min(5, nsw - 1 - done);  // dump depth: 9 states = 5 + 4
+            const int t = std::min(kMaxDumpDepth, nsw - 1 - done);  // dump depth: 9 states = 5 + 4
             PassTable tab;
             memset(&tab, 0, sizeof(tab));
             tab.npairs = n;
@@ -819,7 +843,7 @@ static hs_status train_backward(const hs_train_pair *pairs, const PairBufs *bufs
         tab.wc = rc.wc;
         long rows = 0;
         for (int i = 0; i < n; ++i) rows += (long)((pairs[i].W + strip_cols_for(tb) - 1) / strip_cols_for(tb)) * pairs[i].H;
-        const long target = (long)sm_count() * kWarpsPerBlock * adj_min_blocks(tb);
+        const long target = (long)sm_count() * adj_res_warps(tb);
         int Lr = (int)std::max(1L, (rows + target - 1) / target);
         Lr = std::max(Lr, std::max(8, 2 * tb));
         tab.item_prefix[0] = 0;
