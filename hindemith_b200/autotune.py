@@ -23,8 +23,8 @@ T_CANDIDATES = (1, 2, 3, 4, 5, 6, 7, 8)
 
 def _seg_candidates(H: int, W: int, T: int):
     out = {0}
-    for L in (16, 32, 64, 128, 256):
-        if L < H:
+    for L in (12, 16, 20, 24, 32, 48, 64, 128, 256):
+        if 2 * T <= L < H:
             out.add(L)
     return sorted(out)
 
