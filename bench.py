@@ -1090,7 +1090,8 @@ def main():
     peak, peak_kind = load_peaks()
     launch_s = t_sweeps / (args.steps * passes)
     achieved = BYTES_PER_PX_PASS * H * W / launch_s / 1e9
-    kernel = (f"hs_stream_w_kernel<{T}>" if wide else
+    # the wide kernel's main loop is unrolled from 3 Mpx up (kWideUnrollPixels in hs_sweep.cu)
+    kernel = (f"hs_stream_w_kernel<{T},{'true' if H * W >= 3000000 else 'false'}>" if wide else
               f"hs_stream_kernel<{T},{'false' if args.exact else 'true'}>")
     # ncu figures of this very kernel at this shape (profiles/), when one was captured
     traffic, prof = None, {}

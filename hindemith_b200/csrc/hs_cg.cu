@@ -25,7 +25,8 @@ constexpr int kMpHalo = 4;                         // >= depth; keeps chunks 16-
 constexpr int kMpStrip = kMpCols - 2 * kMpHalo;    // output columns per strip
 constexpr int kMpPrefetch = 2;                     // rows in flight per warp
 constexpr int kMpPlanes = 4;                       // u, v, Ix, Iy
-constexpr int kMpWarps = 4;                        // warps per CTA
+constexpr int kMpWarps = 1;                        // warps per CTA (each warp is a work item)
+constexpr int kMpResWarps = 12;                    // resident warps per SM the registers allow
 
 template <int D>
 struct MpGeo {
@@ -77,17 +78,18 @@ __device__ __forceinline__ float f4at(const float4 &a, int j) {
     return j == 0 ? a.x : (j == 1 ? a.y : (j == 2 ? a.z : a.w));
 }
 
-// three CTAs (12 warps) per SM: the depth-4 pass needs 167 registers and 57 KB of shared
-// memory per CTA
-constexpr int kMpBlocksPerSm = 3;
-
+// 12 warps per SM: the depth-4 pass needs up to 168 registers and 14 KB of shared memory per
+// warp.  One-warp CTAs free a slot as soon as its item ends; under programmatic dependent
+// launch the next pass's items take it while the rest of this pass finishes.
 template <int D>
-__global__ void __launch_bounds__(kMpWarps * 32, kMpBlocksPerSm) mp_stream_kernel(const MpParams p) {
+__global__ void __launch_bounds__(kMpWarps * 32, kMpResWarps / kMpWarps) mp_stream_kernel(const MpParams p) {
     using G = MpGeo<D>;
     extern __shared__ float4 sm4[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     float *ring = reinterpret_cast<float *>(sm4) + warp * G::warp_floats;
+    griddep_launch_dependents();
+    griddep_wait();  // the previous pass (its powers are this pass's input) has completed
     const int item = blockIdx.x * kMpWarps + warp;
     if (item >= p.nitems) return;  // warp-uniform
     const int strip = item % p.nstrips, seg = item / p.nstrips;
@@ -188,9 +190,17 @@ static hs_status launch_mp(const MpParams &pp, cudaStream_t s) {
                                            MpGeo<D>::smem_bytes));
         attr[dev] = true;
     }
-    const unsigned blocks = (unsigned)((pp.nitems + kMpWarps - 1) / kMpWarps);
-    mp_stream_kernel<D><<<blocks, kMpWarps * 32, MpGeo<D>::smem_bytes, s>>>(pp);
-    HS_LAUNCH_CHECK("mp_stream_kernel");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((pp.nitems + kMpWarps - 1) / kMpWarps));
+    cfg.blockDim = dim3(kMpWarps * 32);
+    cfg.dynamicSmemBytes = MpGeo<D>::smem_bytes;
+    cfg.stream = s;
+    cudaLaunchAttribute a[1];
+    a[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    a[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = a;
+    cfg.numAttrs = 1;
+    HS_CUDA_CHECK(cudaLaunchKernelEx(&cfg, mp_stream_kernel<D>, pp));
     return HS_OK;
 }
 
@@ -275,7 +285,7 @@ hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const fl
     const size_t row = (size_t)W * sizeof(float), pitch = (size_t)ld * sizeof(float);
     // segments: about one wave of resident warps over all strips, at least 8 rows
     const int nstrips = (W + kMpStrip - 1) / kMpStrip;
-    const long target = (long)sm_count() * kMpWarps * kMpBlocksPerSm;
+    const long target = (long)sm_count() * kMpResWarps;
     const long nseg = std::max(1L, (target + nstrips - 1) / nstrips);
     const int seg_rows = std::min(H, std::max(8, (int)((H + nseg - 1) / nseg)));
     const int nitems = nstrips * ((H + seg_rows - 1) / seg_rows);

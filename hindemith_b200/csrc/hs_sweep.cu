@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(kPassWarps * 32, res_warps(T) / kPassWarps)
 // The fast form in the wide layout (hs_stream4.cuh).
 constexpr int res_warps_w(int T) { return T <= 4 ? 12 : 8; }
 
-template <int T>
+template <int T, bool UNR>
 __global__ void __launch_bounds__(kPassWarps * 32, res_warps_w(T) / kPassWarps)
     hs_stream_w_kernel(const SweepParams p) {
     extern __shared__ float4 smem4[];
@@ -47,7 +47,7 @@ __global__ void __launch_bounds__(kPassWarps * 32, res_warps_w(T) / kPassWarps)
     if (item >= p.nitems) return;  // warp-uniform
     ItemW it;
     init_item_w<T>(it, p, item % p.nstrips, item / p.nstrips, lane, wbase);
-    run_item_w<T>(p, it);
+    run_item_w<T, false, UNR>(p, it);
 }
 
 // ------------------------------------------------------------------ host side
@@ -76,11 +76,17 @@ static hs_status launch_kernel(KernelFn fn, int smem, bool *attr_set, const Swee
     return HS_OK;
 }
 
+// Images below this size (L2-resident) run the wide kernel's main loop rolled, larger ones
+// unrolled two steps (stream_item_w).
+constexpr long kWideUnrollPixels = 3000000;
+
 template <int T>
 static hs_status launch_one_w(const SweepParams &pp, cudaStream_t stream) {
-    static bool attr_set[64] = {};
-    return launch_kernel(hs_stream_w_kernel<T>, kPassWarps * GeoW<T>::warp_floats * (int)sizeof(float),
-                         attr_set, pp, stream);
+    static bool attr_set[64] = {}, attr_set_r[64] = {};
+    constexpr int smem = kPassWarps * GeoW<T>::warp_floats * (int)sizeof(float);
+    if ((long)pp.H * pp.W >= kWideUnrollPixels)
+        return launch_kernel(hs_stream_w_kernel<T, true>, smem, attr_set, pp, stream);
+    return launch_kernel(hs_stream_w_kernel<T, false>, smem, attr_set_r, pp, stream);
 }
 
 int strip_cols_wide(int T) {

@@ -233,6 +233,22 @@ def test_wide_layout_equals_narrow(cuda, shape, T):
         assert_bitexact(got[1], ref[1], "v")
 
 
+@pytest.mark.parametrize("shape", [(1544, 2040), (1543, 2043)])
+@pytest.mark.parametrize("T", ALL_T)
+def test_wide_layout_equals_narrow_large(cuda, shape, T):
+    """From 3 Mpx up the wide kernel runs its main loop unrolled two steps, a separate
+    instantiation from the rolled loop of the smaller shapes above: bit-identical to the
+    2-column layout there too (W % 4 == 0 and not)."""
+    H, W = shape
+    assert H * W >= 3000000
+    rng = np.random.default_rng(H + W + T)
+    Ix, Iy, It, u0, v0 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(5))
+    ref = run_sweeps(Ix, Iy, It, 0.8, 23, u0, v0, sweeps_per_pass=T, fast_math=True, layout=1)
+    got = run_sweeps(Ix, Iy, It, 0.8, 23, u0, v0, sweeps_per_pass=T, fast_math=True, layout=2)
+    assert_bitexact(got[0], ref[0], "u")
+    assert_bitexact(got[1], ref[1], "v")
+
+
 def test_wide_layout_full_size(cuda):
     """1920x1080, 60 sweeps: the automatic layout (wide at this size) equals the narrow one
     and stays within 1e-4 of FP64."""
