@@ -329,7 +329,9 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     }
 }
 
-template <int T, bool FAST, bool XEDGE, bool DUMP>
+// UNR: the main loop body holds two steps; the per-pass kernel runs it rolled on
+// L2-resident images from depth 3 up, where the shorter code measured faster (hs_sweep.cu).
+template <int T, bool FAST, bool XEDGE, bool DUMP, bool UNR = true>
 __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it) {
     const int k0 = max(0, it.y_start - T);
     const int k_end = it.y_end - 1 + T;
@@ -365,11 +367,16 @@ __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it
     }
     if (klo + 1 <= khi) {
         for (; k < klo; advance()) stream_step<T, FAST, XEDGE, true, DUMP>(p, it, w, k, rslot, cslot);
-        while (k + 1 <= khi) {
-            stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
-            advance();
-            stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
-            advance();
+        if constexpr (UNR) {
+            while (k + 1 <= khi) {
+                stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
+                advance();
+                stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
+                advance();
+            }
+        } else {
+#pragma unroll 1
+            for (; k <= khi; advance()) stream_step<T, FAST, XEDGE, false, DUMP>(p, it, w, k, rslot, cslot);
         }
         // Here k <= H-1, so row H-1 reaches every stage in the tail loop below.  The
         // bottom-clamp values are written and read only there; dropping the head loop's
@@ -443,11 +450,11 @@ __device__ __forceinline__ void init_item(Item &it, const SweepParams &p, int st
 // Run one work item; only strips reaching an image side need the horizontal clamps.
 // DUMP (the training recompute) also writes every stage's sweep to p.dump_u/v; it is a
 // template parameter so the plain kernels carry no per-stage branch.
-template <int T, bool FAST, bool DUMP = false>
+template <int T, bool FAST, bool DUMP = false, bool UNR = true>
 __device__ __forceinline__ void run_item(const SweepParams &p, const Item &it) {
     const int x0 = it.xa - 2 * it.lane;
-    if (x0 <= 0 || x0 + kWarpCols >= p.W) stream_item<T, FAST, true, DUMP>(p, it);
-    else stream_item<T, FAST, false, DUMP>(p, it);
+    if (x0 <= 0 || x0 + kWarpCols >= p.W) stream_item<T, FAST, true, DUMP, UNR>(p, it);
+    else stream_item<T, FAST, false, DUMP, UNR>(p, it);
 }
 
 }  // namespace hs

@@ -11,7 +11,7 @@ namespace hs {
 // (Measured: capping registers for more warps costs more ILP than it gains.)
 constexpr int res_warps(int T) { return T <= 4 ? 16 : (T <= 6 ? 12 : 8); }
 
-template <int T, bool FAST>
+template <int T, bool FAST, bool UNR>
 __global__ void __launch_bounds__(kPassWarps * 32, res_warps(T) / kPassWarps)
     hs_stream_kernel(const SweepParams p) {
     extern __shared__ float4 smem4[];
@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(kPassWarps * 32, res_warps(T) / kPassWarps)
     if (item >= p.nitems) return;  // warp-uniform
     Item it;
     init_item<T>(it, p, item % p.nstrips, item / p.nstrips, lane, wbase);
-    run_item<T, FAST>(p, it);
+    run_item<T, FAST, false, UNR>(p, it);
 }
 
 // The fast form in the wide layout (hs_stream4.cuh).
@@ -76,15 +76,15 @@ static hs_status launch_kernel(KernelFn fn, int smem, bool *attr_set, const Swee
     return HS_OK;
 }
 
-// Images below this size (L2-resident) run the wide kernel's main loop rolled, larger ones
-// unrolled two steps (stream_item_w).
-constexpr long kWideUnrollPixels = 3000000;
+// Images below this size (L2-resident) run the sweep kernels' main loop rolled, larger ones
+// unrolled two steps (stream_item_w, stream_item).
+constexpr long kUnrollPixels = 3000000;
 
 template <int T>
 static hs_status launch_one_w(const SweepParams &pp, cudaStream_t stream) {
     static bool attr_set[64] = {}, attr_set_r[64] = {};
     constexpr int smem = kPassWarps * GeoW<T>::warp_floats * (int)sizeof(float);
-    if ((long)pp.H * pp.W >= kWideUnrollPixels)
+    if ((long)pp.H * pp.W >= kUnrollPixels)
         return launch_kernel(hs_stream_w_kernel<T, true>, smem, attr_set, pp, stream);
     return launch_kernel(hs_stream_w_kernel<T, false>, smem, attr_set_r, pp, stream);
 }
@@ -119,8 +119,13 @@ static hs_status launch_pass_w(int T, const SweepParams &pp, cudaStream_t s) {
 template <int T, bool FAST>
 static hs_status launch_one(const SweepParams &pp, cudaStream_t stream) {
     using G = Geo<T>;
-    auto fn = hs_stream_kernel<T, FAST>;
-    static bool attr_set[64] = {};
+    // rolled main loop from depth 3 on images below kUnrollPixels (measured on B200,
+    // 1080p x 500: exact T = 4 262 against 257 Gpix-it/s, T = 5 225 against 200, fast T = 4
+    // 391 against 359; at T = 2 the unrolled loop is faster, 251 against 211)
+    const bool roll = T >= 3 && (long)pp.H * pp.W < kUnrollPixels;
+    auto fn = roll ? hs_stream_kernel<T, FAST, false> : hs_stream_kernel<T, FAST, true>;
+    static bool attr_set_u[64] = {}, attr_set_r[64] = {};
+    bool *attr_set = roll ? attr_set_r : attr_set_u;
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !attr_set[dev]) {

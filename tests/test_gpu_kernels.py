@@ -249,6 +249,19 @@ def test_wide_layout_equals_narrow_large(cuda, shape, T):
     assert_bitexact(got[1], ref[1], "v")
 
 
+@pytest.mark.parametrize("T", ALL_T)
+def test_exact_form_large_equals_the_oracle(cuda, T):
+    """From 3 Mpx up the 2-column kernel runs its main loop unrolled two steps (below, rolled
+    from depth 3): the exact form still equals the FP32 C oracle bit for bit."""
+    H, W = 1543, 2043
+    rng = np.random.default_rng(7 + T)
+    Ix, Iy, It, u0, v0 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(5))
+    got = run_sweeps(Ix, Iy, It, 0.8, 2 * T + 1, u0, v0, sweeps_per_pass=T, fast_math=False)
+    ru, rv = O.c_hs_sweeps(Ix, Iy, It, 0.8, 2 * T + 1, u0, v0)
+    assert_bitexact(got[0], ru, "u")
+    assert_bitexact(got[1], rv, "v")
+
+
 def test_wide_layout_full_size(cuda):
     """1920x1080, 60 sweeps: the automatic layout (wide at this size) equals the narrow one
     and stays within 1e-4 of FP64."""
