@@ -58,7 +58,7 @@ def _save_file():
             pass
 
 
-def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=3, layout=0):
+def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=5, layout=0):
     import torch
 
     from . import _lib as L
@@ -99,7 +99,9 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
     for p in planes:
         p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
     Ix, Iy, It, u, v = planes
-    sweeps = 120  # the same sweep count for every candidate (a partial last pass at T = 7)
+    # the same sweep count for every candidate: whole passes at depths 1-6 and 8, one partial
+    # at 7 (candidates 1-2 % apart, such as T = 6 and 7 at 1080p, need the longer run)
+    sweeps = 240
     results = []
     for layout in ((1, 2) if fast_math else (1,)):
         for T in candidates:
