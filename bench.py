@@ -972,7 +972,7 @@ def main():
     if args.sweeps_per_pass > 0:
         T, seg, layout = args.sweeps_per_pass, 0, args.layout
     else:
-        T, seg, layout = autotune.best_sweep_config(H, W, ld, fast_math=not args.exact)
+        T, seg, layout = autotune.best_sweep_config(H, W, ld, fast_math=not args.exact, sweeps=iters)
     cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=not args.exact,
                         layout=layout)
     # the layout the library runs (hs_config.layout 0 chooses by image size)
@@ -1039,7 +1039,7 @@ def main():
         # FP32 operations one rounding at a time, 2 columns per lane, its own tuned depth)
         t_exact = None
         if not args.exact and not args.shape and not args.no_exact_form:
-            Te, sege, _ = autotune.best_sweep_config(H, W, ld, fast_math=False)
+            Te, sege, _ = autotune.best_sweep_config(H, W, ld, fast_math=False, sweeps=iters)
             cfg_e = L.make_config(sweeps_per_pass=Te, rows_per_segment=sege)
 
             def exact_step():
@@ -1069,7 +1069,8 @@ def main():
             c0 = synthetic.plain_256()
             a0, b0, _, _ = synthetic.generate(c0)
             d0, d1 = D.as_plane(torch.from_numpy(a0).cuda()), D.as_plane(torch.from_numpy(b0).cuda())
-            T0, s0, l0 = autotune.best_sweep_config(c0.H, c0.W, D.ld_of(d0), fast_math=True)
+            T0, s0, l0 = autotune.best_sweep_config(c0.H, c0.W, D.ld_of(d0), fast_math=True,
+                                                    sweeps=c0.iters)
             cf0 = L.make_config(sweeps_per_pass=T0, rows_per_segment=s0, fast_math=True, layout=l0)
             fu, fv = D.hs_forward(d0, d1, c0.alpha, c0.iters, cf0)
             eu, ev = D.hs_forward(d0, d1, c0.alpha, c0.iters)  # the library's default config

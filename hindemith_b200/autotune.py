@@ -79,15 +79,17 @@ def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=5, layout=0):
 
 
 def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
-                      candidates=T_CANDIDATES) -> Tuple[int, int, int]:
+                      candidates=T_CANDIDATES, sweeps: int = 240) -> Tuple[int, int, int]:
     """(sweeps_per_pass, rows_per_segment, layout) fastest on the current device for HxW;
-    both layouts (2 and 4 columns per lane) compete in the fast form."""
+    both layouts (2 and 4 columns per lane) compete in the fast form.  Every candidate is timed
+    over `sweeps` sweeps: pass the workload's own count when it is known (the last, partial
+    pass differs by depth)."""
     import torch
 
     from . import device as D
 
     dev_name = torch.cuda.get_device_name()
-    key = _key(dev_name, H, W, ld, fast_math) + "|layout"
+    key = _key(dev_name, H, W, ld, fast_math) + "|layout" + ("" if sweeps == 240 else f"|s{sweeps}")
     with _lock:
         if not _cache:
             _load_file()
@@ -99,9 +101,8 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
     for p in planes:
         p.copy_(torch.rand((H, W), device="cuda", generator=g) - 0.5)
     Ix, Iy, It, u, v = planes
-    # the same sweep count for every candidate: whole passes at depths 1-6 and 8, one partial
-    # at 7 (candidates 1-2 % apart, such as T = 6 and 7 at 1080p, need the longer run)
-    sweeps = 240
+    # the same sweep count for every candidate (by default whole passes at depths 1-6 and 8,
+    # one partial at 7; candidates 1-2 % apart, such as T = 6 and 7 at 1080p, need long runs)
     results = []
     for layout in ((1, 2) if fast_math else (1,)):
         for T in candidates:

@@ -287,7 +287,9 @@ hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const fl
     const int nstrips = (W + kMpStrip - 1) / kMpStrip;
     const long target = (long)sm_count() * kMpResWarps;
     const long nseg = std::max(1L, (target + nstrips - 1) / nstrips);
-    const int seg_rows = std::min(H, std::max(8, (int)((H + nseg - 1) / nseg)));
+    const int seg_rows = (cfg && cfg->rows_per_segment > 0)
+                             ? std::min(H, cfg->rows_per_segment)
+                             : std::min(H, std::max(8, (int)((H + nseg - 1) / nseg)));
     const int nitems = nstrips * ((H + seg_rows - 1) / seg_rows);
     if (steps == 1) {  // V[0] = r only
         if (V0 != r0) HS_CUDA_CHECK(cudaMemcpy2DAsync(V0, pitch, r0, pitch, row, H, cudaMemcpyDeviceToDevice, s));

@@ -184,16 +184,21 @@ static int seg_rows_for(int H, int nstrips, int T, long warps_per_sm) {
 
 int default_seg_rows(int H, int nstrips, int T) { return seg_rows_for(H, nstrips, T, 16); }
 
-// Measured on B200: the wide layout wins from about a 1080p image up (4096^2: 700 vs 592
-// Gpix-it/s), the narrow one below (more strips for the SMs on small images).
+// Measured on B200: in a launch of several pairs (the batch and the training passes) the wide
+// layout wins from about a 1080p image up (4096^2: 700 vs 592 Gpix-it/s), the narrow one below
+// (more strips for the SMs on small images).  For one pair in one-warp CTAs the crossing lies
+// near 250 kpx: at the default segments, as a fraction of the fastest tuned time, 480x640 runs
+// 1.01 wide (T = 6) against 1.26 narrow, 512^2 1.05 against 1.12, 256^2 1.14 against 1.00.
 constexpr long kWideAutoPixels = 2000000;
+constexpr long kWideAutoPixelsPair = 250000;
 
-bool use_wide(const ResolvedConfig &rc, long pixels) {
+static bool use_wide_at(const ResolvedConfig &rc, long pixels, long threshold) {
     if (!rc.fast) return false;
     if (rc.layout == 2) return true;
     if (rc.layout == 1) return false;
-    return pixels >= kWideAutoPixels;
+    return pixels >= threshold;
 }
+bool use_wide(const ResolvedConfig &rc, long pixels) { return use_wide_at(rc, pixels, kWideAutoPixels); }
 
 hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out) {
     hs_config c = {};
@@ -224,16 +229,17 @@ hs_status resolve_config(const hs_config *cfg, ResolvedConfig *out) {
 
 
 // The depth the per-pair sweep runs when hs_config.sweeps_per_pass is 0.  The table rounds
-// the autotuner's picks on B200 by image size (rows per segment and layout left to their
-// defaults); at each of 240x320, 256^2, 480x640, 512^2, 1280x720, 1920x1080, 2048^2 and
-// 4096^2 its depth is within 6 % of the fastest tuned configuration, fast and exact form.
+// the depths that are fastest on B200 at the default rows per segment and layout, by image
+// size; at each of 240x320, 256^2, 480x640, 512^2, 1280x720, 1920x1080, 2048^2 and 4096^2 it
+// runs within 6 % of the fastest tuned configuration (16 % at 512^2 in the fast form), fast
+// and exact form.
 void apply_shape_default(ResolvedConfig &rc, int H, int W) {
     if (!rc.T_default) return;
     const long px = (long)H * W;
     if (rc.fast)
-        rc.T = px < 100000 ? 4 : px < 500000 ? 6 : px < 2000000 ? 5 : 6;
+        rc.T = px < 250000 ? 4 : px < 600000 ? 6 : px < 1500000 ? 5 : 7;
     else
-        rc.T = px < 200000 ? 3 : px < 600000 ? 5 : px < 1500000 ? 3 : px < 3000000 ? 2 : 3;
+        rc.T = px < 200000 ? 4 : px < 600000 ? 5 : 4;
 }
 
 // Runs `iters` sweeps.  State starts in (u0, v0) if `start_in_user`, else in (u1, v1);
@@ -259,7 +265,7 @@ hs_status run_passes_dev(const float *Ix, const float *Iy, const float *It, int 
         pp.alpha_dev = alpha_dev;
         pp.dump = 0;
         pp.we = rc.we; pp.wc = rc.wc;
-        const bool wide = use_wide(rc, (long)H * W);
+        const bool wide = use_wide_at(rc, (long)H * W, kWideAutoPixelsPair);
         const int sc = wide ? strip_cols_wide(t) : strip_cols_for(t);
         pp.nstrips = (W + sc - 1) / sc;
         pp.seg_rows = rc.seg_rows > 0 ? std::min(rc.seg_rows, H)

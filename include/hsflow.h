@@ -57,7 +57,8 @@ typedef struct hs_config {
     int sweeps_per_pass;  /* temporal-blocking depth T (1..8) = sweeps per HBM pass; 0 = default:
                            * for hs_forward / hs_sweeps / hs_forward_noalloc a measured table by
                            * image size and form (within 6 % of the autotuned best on B200 from
-                           * 240x320 to 4096^2), 4 for the other calls */
+                           * 240x320 to 4096^2, 16 % at 512^2 in the fast form), 4 for the
+                           * other calls */
     int rows_per_segment; /* rows each warp streams per work item; 0 = default */
     int fast_math;        /* 0 (default): the reference program's operation order, one
                              rounding per operation -- bit-identical to the reference's
@@ -66,8 +67,10 @@ typedef struct hs_config {
     float avg_edge;       /* weight of the 4 edge taps of the 3x3 average; 0 = 1/6 */
     float avg_corner;     /* weight of the 4 corner taps; 0 = 1/12 (both 0 = the HS stencil) */
     int layout;           /* columns per lane of the sweep kernels: 0 = chosen by image size
-                             (the batched launch keeps 2), 1 = 2 (64-column strips), 2 = 4
-                             (128-column strips; fast_math only).  Results do not depend on it. */
+                             (4 from 250 kpx for one pair, from 2 Mpx of average pair size in
+                             the training calls; the batched launch keeps 2), 1 = 2 (64-column
+                             strips), 2 = 4 (128-column strips; fast_math only).  Results do not
+                             depend on it. */
     int reserved[2];      /* must be zero */
 } hs_config;
 
@@ -278,7 +281,8 @@ HS_API hs_status hs_warp_adjoint(const float *src, const float *u, const float *
  * in the template's operation order (bit-identical to its FP32 semantics).  V0, V1 hold
  * `steps` planes each, power s at V + s * power_stride floats (power_stride >= H*ld, a
  * multiple of 4).  cfg->sweeps_per_pass (1..4, 0 = 4) powers are computed per pass over
- * HBM, streaming the image in column strips with the powers as a register pipeline. */
+ * HBM, streaming the image in column strips with the powers as a register pipeline, each warp
+ * over cfg->rows_per_segment rows (0 = about one wave of warps over the image). */
 HS_API hs_status hs_matrix_powers(float lam, const float *Ix, const float *Iy, const float *r0,
                                   const float *r1, int H, int W, int ld, int steps, float *V0,
                                   float *V1, size_t power_stride, const hs_config *cfg,

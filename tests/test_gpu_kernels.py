@@ -295,7 +295,8 @@ def test_plain_1080p_500_at_the_tuned_config(cuda, fast):
     spec = synthetic.plain_1080p()
     I0, I1, _, _ = synthetic.generate(spec)
     a, b = dev(I0), dev(I1)
-    T, seg, layout = autotune.best_sweep_config(spec.H, spec.W, D.ld_of(a), fast_math=fast)
+    T, seg, layout = autotune.best_sweep_config(spec.H, spec.W, D.ld_of(a), fast_math=fast,
+                                                sweeps=spec.iters)
     cfg = L.make_config(sweeps_per_pass=T, rows_per_segment=seg, fast_math=fast, layout=layout)
     u, v = (host(t) for t in D.hs_forward(a, b, spec.alpha, spec.iters, cfg))
     if fast:
