@@ -33,6 +33,15 @@ def _key(dev_name, H, W, ld, fast_math):
     return f"{dev_name}|{H}x{W}|ld{ld}|{'fast' if fast_math else 'exact'}"
 
 
+DEFAULT_TUNING_SWEEPS = 240
+
+
+def _sweep_key(dev_name, H, W, ld, fast_math, sweeps):
+    """Cache key of a sweep tuning; a run over another sweep count is cached apart."""
+    key = _key(dev_name, H, W, ld, fast_math) + "|layout"
+    return key if sweeps == DEFAULT_TUNING_SWEEPS else key + f"|s{sweeps}"
+
+
 def _file():
     return os.environ.get("HS_AUTOTUNE_CACHE")
 
@@ -79,7 +88,8 @@ def time_config(Ix, Iy, It, u, v, T, seg, fast_math, sweeps, reps=5, layout=0):
 
 
 def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
-                      candidates=T_CANDIDATES, sweeps: int = 240) -> Tuple[int, int, int]:
+                      candidates=T_CANDIDATES,
+                      sweeps: int = DEFAULT_TUNING_SWEEPS) -> Tuple[int, int, int]:
     """(sweeps_per_pass, rows_per_segment, layout) fastest on the current device for HxW;
     both layouts (2 and 4 columns per lane) compete in the fast form.  Every candidate is timed
     over `sweeps` sweeps: pass the workload's own count when it is known (the last, partial
@@ -89,7 +99,7 @@ def best_sweep_config(H: int, W: int, ld: int, fast_math: bool = True,
     from . import device as D
 
     dev_name = torch.cuda.get_device_name()
-    key = _key(dev_name, H, W, ld, fast_math) + "|layout" + ("" if sweeps == 240 else f"|s{sweeps}")
+    key = _sweep_key(dev_name, H, W, ld, fast_math, sweeps)
     with _lock:
         if not _cache:
             _load_file()
