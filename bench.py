@@ -1091,12 +1091,12 @@ def main():
     peak, peak_kind = load_peaks()
     launch_s = t_sweeps / (args.steps * passes)
     achieved = BYTES_PER_PX_PASS * H * W / launch_s / 1e9
-    # the sweep kernels' main loop is unrolled from 3 Mpx up (kUnrollPixels in hs_sweep.cu),
-    # and the 2-column kernel's also at depths 1 and 2
+    # the wide kernel's main loop is unrolled from 3 Mpx up (kUnrollPixels in hs_sweep.cu),
+    # the 2-column kernel's at depths 1 and 2
     big = H * W >= 3000000
     kernel = (f"hs_stream_w_kernel<{T},{'true' if big else 'false'}>" if wide else
               f"hs_stream_kernel<{T},{'false' if args.exact else 'true'},"
-              f"{'true' if big or T <= 2 else 'false'}>")
+              f"{'true' if T <= 2 else 'false'}>")
     # ncu figures of this very kernel at this shape (profiles/), when one was captured
     traffic, prof = None, {}
     tpath = os.path.join(HERE, "profiles", "sweep_traffic.json")

@@ -329,8 +329,8 @@ __device__ __forceinline__ void stream_step(const SweepParams &p, const Item &it
     }
 }
 
-// UNR: the main loop body holds two steps; the per-pass kernel runs it rolled on
-// L2-resident images from depth 3 up, where the shorter code measured faster (hs_sweep.cu).
+// UNR: the main loop body holds two steps; the per-pass kernel runs it rolled from depth 3 up,
+// where the shorter code measured faster at every image size (hs_sweep.cu).
 template <int T, bool FAST, bool XEDGE, bool DUMP, bool UNR = true>
 __device__ __forceinline__ void stream_item(const SweepParams &p, const Item &it) {
     const int k0 = max(0, it.y_start - T);

@@ -76,8 +76,10 @@ static hs_status launch_kernel(KernelFn fn, int smem, bool *attr_set, const Swee
     return HS_OK;
 }
 
-// Images below this size (L2-resident) run the sweep kernels' main loop rolled, larger ones
-// unrolled two steps (stream_item_w, stream_item).
+// Images below this size (L2-resident) run the wide kernel's main loop rolled, larger ones
+// unrolled two steps (stream_item_w); measured on B200 (fast form, T = 7): 1080p 521 against
+// 502 Gpix-it/s rolled, 2048^2 605 against 608, 2560x1440 536 against 546, 4096^2 900 against
+// 918.
 constexpr long kUnrollPixels = 3000000;
 
 template <int T>
@@ -119,13 +121,12 @@ static hs_status launch_pass_w(int T, const SweepParams &pp, cudaStream_t s) {
 template <int T, bool FAST>
 static hs_status launch_one(const SweepParams &pp, cudaStream_t stream) {
     using G = Geo<T>;
-    // rolled main loop from depth 3 on images below kUnrollPixels (measured on B200,
-    // 1080p x 500: exact T = 4 262 against 257 Gpix-it/s, T = 5 225 against 200, fast T = 4
-    // 391 against 359; at T = 2 the unrolled loop is faster, 251 against 211)
-    const bool roll = T >= 3 && (long)pp.H * pp.W < kUnrollPixels;
-    auto fn = roll ? hs_stream_kernel<T, FAST, false> : hs_stream_kernel<T, FAST, true>;
-    static bool attr_set_u[64] = {}, attr_set_r[64] = {};
-    bool *attr_set = roll ? attr_set_r : attr_set_u;
+    // rolled main loop from depth 3 at every image size (measured on B200, exact form: 1080p
+    // T = 4 262 against 257 Gpix-it/s, T = 5 225 against 200; 2048^2 T = 6 278 against 237;
+    // 3840x2160 T = 6 319 against 295; 4096^2 T = 4 390 against 386; fast form at 1080p T = 4
+    // 391 against 359); at T = 2 the unrolled loop is faster (1080p exact: 251 against 211)
+    auto fn = hs_stream_kernel<T, FAST, (T <= 2)>;
+    static bool attr_set[64] = {};
     int dev = 0;
     cudaGetDevice(&dev);
     if (dev < 64 && !attr_set[dev]) {

@@ -251,8 +251,9 @@ def test_wide_layout_equals_narrow_large(cuda, shape, T):
 
 @pytest.mark.parametrize("T", ALL_T)
 def test_exact_form_large_equals_the_oracle(cuda, T):
-    """From 3 Mpx up the 2-column kernel runs its main loop unrolled two steps (below, rolled
-    from depth 3): the exact form still equals the FP32 C oracle bit for bit."""
+    """A large image (3.15 Mpx) in the exact form, at every depth (the 2-column kernel's main
+    loop rolled from depth 3, unrolled two steps below): equal to the FP32 C oracle bit for
+    bit."""
     H, W = 1543, 2043
     rng = np.random.default_rng(7 + T)
     Ix, Iy, It, u0, v0 = (rng.standard_normal((H, W)).astype(np.float32) for _ in range(5))
