@@ -52,6 +52,31 @@ __global__ void __launch_bounds__(256) blur_down_adjoint_kernel(const float *__r
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int y = blockIdx.y * blockDim.y + threadIdx.y;
     if (x >= W || y >= H) return;
+    // Off the borders (every coarse index the pixel needs exists and no tap is clamped) the
+    // weights are the bare binomial taps: an even fine index p gathers coarse p/2-1, p/2,
+    // p/2+1 with (1, 6, 1)/16, an odd one (p-1)/2 and (p+1)/2 with (4, 4)/16.  The same fused
+    // multiply-adds in the same order as the general loop below, so the same bits.
+    if (x >= 2 && x + 2 <= 2 * Wo - 2 && y >= 2 && y + 2 <= 2 * Ho - 2) {
+        const float b0 = kBin5[0], b1 = kBin5[1], b2 = kBin5[2];
+        const int mx = x >> 1;
+        auto row = [&](int oy) {
+            const float *rp = dout + (size_t)oy * ldo;
+            if (x & 1) return fmaf(b1, __ldg(rp + mx + 1), fmaf(b1, __ldg(rp + mx), 0.f));
+            return fmaf(b0, __ldg(rp + mx + 1), fmaf(b2, __ldg(rp + mx), fmaf(b0, __ldg(rp + mx - 1), 0.f)));
+        };
+        const int my = y >> 1;
+        float acc;
+        if (y & 1) {
+            acc = fmaf(b1, row(my), 0.f);
+            acc = fmaf(b1, row(my + 1), acc);
+        } else {
+            acc = fmaf(b0, row(my - 1), 0.f);
+            acc = fmaf(b2, row(my), acc);
+            acc = fmaf(b0, row(my + 1), acc);
+        }
+        din[(size_t)y * ld + x] = acc;
+        return;
+    }
     const int oy0 = max(0, (y - 3) / 2), oy1 = min(Ho - 1, (y + 3) / 2);
     const int ox0 = max(0, (x - 3) / 2), ox1 = min(Wo - 1, (x + 3) / 2);
     float acc = 0.f;
