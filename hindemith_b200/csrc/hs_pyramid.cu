@@ -230,13 +230,15 @@ __global__ void __launch_bounds__(256) warp_adjoint_scale_kernel(const float *__
                                                                  const float *__restrict__ ov,
                                                                  int H, int W, int ld,
                                                                  unsigned *__restrict__ ws) {
+    // blocks stride over rows, threads over a row's columns (no per-element division); the
+    // maximum does not depend on the order
     unsigned mg = 0u, mf = 0u;
-    const long long n = (long long)H * W;
-    for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < n;
-         e += (long long)gridDim.x * blockDim.x) {
-        const size_t i = (size_t)(e / W) * ld + (size_t)(e % W);
-        mg = max(mg, __float_as_uint(fabsf(__ldg(g + i))));
-        mf = max(mf, max(__float_as_uint(fabsf(__ldg(ou + i))), __float_as_uint(fabsf(__ldg(ov + i)))));
+    for (int y = blockIdx.x; y < H; y += gridDim.x) {
+        const size_t r = (size_t)y * ld;
+        for (int x = threadIdx.x; x < W; x += blockDim.x) {
+            mg = max(mg, __float_as_uint(fabsf(__ldg(g + r + x))));
+            mf = max(mf, max(__float_as_uint(fabsf(__ldg(ou + r + x))), __float_as_uint(fabsf(__ldg(ov + r + x)))));
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -426,8 +428,7 @@ hs_status hs_warp_adjoint(const float *src, const float *u, const float *v, cons
     unsigned *scale = reinterpret_cast<unsigned *>(workspace);
     auto *acc = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(workspace) + 256);
     HS_CUDA_CHECK(cudaMemsetAsync(workspace, 0, need, s));
-    const long long n = (long long)H * W;
-    const int blocks = (int)std::min<long long>((n + 255) / 256, (long long)sm_count() * 8);
+    const int blocks = std::min(H, sm_count() * 8);
     warp_adjoint_scale_kernel<<<std::max(blocks, 1), 256, 0, s>>>(ddst, u, v, H, W, ld, scale);
     HS_LAUNCH_CHECK("warp_adjoint_scale_kernel");
     warp_adjoint_kernel<<<g2(H, W), dim3(64, 4), 0, s>>>(src, u, v, ddst, H, W, ld, scale, acc, du, dv);
